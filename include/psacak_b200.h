@@ -1,0 +1,138 @@
+/*
+ * psacak_b200.h -- C ABI of the B200 suffix-array builder.
+ *
+ * The builder keeps hucsmn/psacak's method (SACA-K L/S typing, LMS
+ * placement, induced L-/S-scans, LMS-substring naming, recursion on the
+ * reduced u32 string, final induction) and runs it as sm_100a CUDA kernels.
+ * Every SA it returns is the suffix array of the input without the sentinel
+ * position, exactly as the reference's src/lib.rs:30-43 documents; a text has
+ * a single such array, so the output is bit-for-bit the reference's.
+ *
+ * All entry points return PSACAK_OK (0) or a negative PSACAK_E* status and
+ * never abort the process; psacak_last_error_string() describes the last
+ * failure on the calling thread.
+ */
+#ifndef PSACAK_B200_H
+#define PSACAK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PSACAK_API __attribute__((visibility("default")))
+#else
+#define PSACAK_API
+#endif
+
+#define PSACAK_OK 0
+#define PSACAK_EINVAL (-1)    /* null pointer, length limit, bad argument */
+#define PSACAK_ENOMEM (-2)    /* device or pinned host allocation failed */
+#define PSACAK_ECUDA (-3)     /* a CUDA runtime call failed */
+#define PSACAK_ETIMEOUT (-4)  /* a bounded device-side wait ran out */
+#define PSACAK_EINTERNAL (-5) /* a device-side consistency check failed */
+
+/* Induced-scan engine selection (psacak_schedule.engine). */
+#define PSACAK_ENGINE_AUTO 0     /* bucket scan for byte levels, doubling otherwise */
+#define PSACAK_ENGINE_BUCKET 1   /* bucket-ordered scan (alphabets <= 256 only) */
+#define PSACAK_ENGINE_DOUBLING 2 /* chain-doubling scan (any alphabet) */
+
+/* Tunables of one build.  Zero fields mean "use the default".  Every
+ * schedule gives the same suffix array; it only changes speed. */
+typedef struct {
+    uint32_t engine;          /* PSACAK_ENGINE_* for level 0 */
+    uint32_t inner_engine;    /* PSACAK_ENGINE_* for levels >= 1 */
+    uint32_t radix_ctas_per_sm; /* CTAs per SM of the radix/scan kernels */
+    uint32_t small_level;     /* levels shorter than this use the small-level path */
+    uint32_t reserved[4];
+} psacak_schedule;
+
+/* One record per recursion level of the last build on a context. */
+typedef struct {
+    uint32_t level;  /* 0 = input text */
+    uint32_t width;  /* symbol width in bytes of this level: 1 or 4 */
+    uint64_t m;      /* level length */
+    uint64_t n_lms;  /* LMS positions = length of the reduced string */
+    uint64_t k;      /* distinct LMS-substring names */
+    uint64_t hash;   /* hash of the translated reduced string (0 when k == n_lms) */
+} psacak_level_info;
+
+typedef struct psacak_ctx psacak_ctx;
+
+/* Creates a builder context on CUDA device `device`.  A context owns a
+ * stream, a grow-only device workspace and a pinned staging buffer; calls
+ * on one context are serialised, distinct contexts are independent. */
+PSACAK_API int psacak_ctx_create(int device, psacak_ctx **out);
+PSACAK_API int psacak_ctx_destroy(psacak_ctx *ctx);
+
+/* Description of the last error on the calling thread ("" if none). */
+PSACAK_API const char *psacak_last_error_string(void);
+
+/* Library version, e.g. "0.1.0". */
+PSACAK_API const char *psacak_version(void);
+
+/*
+ * psacak8 -- suffix array of a byte string, host pointers.
+ * Replaces psacak_inplace(text: &[u8], suf: &mut [u32]) (src/lib.rs:77-82)
+ * and psacak (src/lib.rs:64-69), which drive psacak8 (src/psacak8.rs:19).
+ * `sa` receives n entries.  n must be < 2^32 - 1 (src/lib.rs:65, :79);
+ * PSACAK_EINVAL otherwise.  Uses a per-thread default context on device 0.
+ */
+PSACAK_API int psacak8(const uint8_t *text, uint64_t n, uint32_t *sa);
+
+/*
+ * psacak32 -- suffix array of an integer-alphabet string, host pointers.
+ * Replaces the reference's integer-alphabet path: translate_sample
+ * (src/psacak32.rs:912-943) followed by psacak32 (src/psacak32.rs:24), with
+ * saca_tiny when distinct symbols >= n (src/psacak32.rs:873-881).  The
+ * translation runs on the device.  n must be <= 2^31 - 1
+ * (src/psacak32.rs:25).
+ */
+PSACAK_API int psacak32(const uint32_t *text, uint64_t n, uint32_t *sa);
+
+/* Same as psacak8 / psacak32 on an explicit context (host pointers). */
+PSACAK_API int psacak8_ctx(psacak_ctx *ctx, const uint8_t *text, uint64_t n, uint32_t *sa,
+                const psacak_schedule *sched);
+PSACAK_API int psacak32_ctx(psacak_ctx *ctx, const uint32_t *text, uint64_t n, uint32_t *sa,
+                 const psacak_schedule *sched);
+
+/* Device-pointer forms: `d_text` and `d_sa` live on the context's device;
+ * `stream` is a cudaStream_t (NULL = the context's own stream).  The call
+ * returns after the build has finished on that stream. */
+PSACAK_API int psacak8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, uint32_t *d_sa,
+                void *stream, const psacak_schedule *sched);
+PSACAK_API int psacak32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, uint32_t *d_sa,
+                 void *stream, const psacak_schedule *sched);
+
+/*
+ * psacak8_batch -- suffix arrays of n_texts independent byte strings in one
+ * build.  The reference has only the per-text call (src/lib.rs:77); this is
+ * that call applied to every text, with one SA per text in sas[i] (lens[i]
+ * entries each).  Host pointers.
+ */
+PSACAK_API int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *lens,
+                  uint32_t n_texts, uint32_t *const *sas, const psacak_schedule *sched);
+
+/* Per-level records of the last build on `ctx` (see psacak_level_info). */
+PSACAK_API int psacak_get_trace(psacak_ctx *ctx, psacak_level_info *out, uint32_t cap, uint32_t *count);
+
+/*
+ * Device-side suffix-array check (Burkhardt & Kaerkkaeinen, CPM 2003, O(n)):
+ * *ok = 1 iff d_sa is a permutation of [0, n) and adjacent suffixes are in
+ * order.  The reference's CLI check (src/bin/psacak.rs:73-80) is the
+ * quadratic form of the same test.
+ */
+PSACAK_API int psacak_check_sa8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n,
+                         const uint32_t *d_sa, int *ok, void *stream);
+PSACAK_API int psacak_check_sa32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n,
+                          const uint32_t *d_sa, int *ok, void *stream);
+
+/* Number of kernels the library launched since the context was created. */
+PSACAK_API uint64_t psacak_kernel_launches(psacak_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,271 @@
+"""psacak_b200 -- pSACAK suffix-array construction on an NVIDIA B200.
+
+Python mirror of hucsmn/psacak's public API (src/lib.rs):
+
+* ``psacak(text) -> numpy.ndarray[uint32]``        (src/lib.rs:64)
+* ``psacak_inplace(text, suf)``                   (src/lib.rs:77)
+* ``psacak32(symbols) -> numpy.ndarray[uint32]``  (integer alphabet; the
+  reference's translate_sample + psacak32 path, src/psacak32.rs:873-943)
+
+Like the reference, the suffix array excludes the sentinel position, and the
+same length limits apply (``len < 2**32 - 1`` for bytes, ``<= 2**31 - 1``
+for integer symbols).  Where the reference panics, these functions raise
+``ValueError``.  Every call runs on the GPU through the C ABI in
+``lib/libpsacak_b200.so``; there is no CPU fallback, and importing the
+functions without the built library raises ``ImportError`` on first use.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+__all__ = [
+    "psacak", "psacak_inplace", "psacak32", "Context", "Schedule", "PsacakError",
+    "ENGINE_AUTO", "ENGINE_BUCKET", "ENGINE_DOUBLING", "lib", "library_path",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "lib", "libpsacak_b200.so")
+
+PSACAK_OK = 0
+PSACAK_EINVAL = -1
+PSACAK_ENOMEM = -2
+PSACAK_ECUDA = -3
+PSACAK_ETIMEOUT = -4
+PSACAK_EINTERNAL = -5
+
+ENGINE_AUTO = 0
+ENGINE_BUCKET = 1
+ENGINE_DOUBLING = 2
+
+_ERRNAMES = {
+    PSACAK_EINVAL: "EINVAL", PSACAK_ENOMEM: "ENOMEM", PSACAK_ECUDA: "ECUDA",
+    PSACAK_ETIMEOUT: "ETIMEOUT", PSACAK_EINTERNAL: "EINTERNAL",
+}
+
+
+class PsacakError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (_ERRNAMES.get(code, "E?"), code, msg))
+        self.code = code
+
+
+class Schedule(ctypes.Structure):
+    """Tunables of one build (psacak_schedule).  Every schedule yields the
+    same suffix array; only the speed differs."""
+    _fields_ = [
+        ("engine", ctypes.c_uint32),
+        ("inner_engine", ctypes.c_uint32),
+        ("radix_ctas_per_sm", ctypes.c_uint32),
+        ("small_level", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
+    ]
+
+
+class LevelInfo(ctypes.Structure):
+    _fields_ = [
+        ("level", ctypes.c_uint32),
+        ("width", ctypes.c_uint32),
+        ("m", ctypes.c_uint64),
+        ("n_lms", ctypes.c_uint64),
+        ("k", ctypes.c_uint64),
+        ("hash", ctypes.c_uint64),
+    ]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def lib():
+    """Loads lib/libpsacak_b200.so (raises ImportError if it is not built)."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError("psacak_b200: %s is not built; run `python -m psacak_b200.build`" % _LIB_PATH)
+        L = ctypes.CDLL(_LIB_PATH)
+        p, u64, u32, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int
+        pp = ctypes.POINTER(ctypes.c_void_p)
+        L.psacak_ctx_create.argtypes = [i32, pp]
+        L.psacak_ctx_destroy.argtypes = [p]
+        L.psacak_last_error_string.restype = ctypes.c_char_p
+        L.psacak_version.restype = ctypes.c_char_p
+        L.psacak8.argtypes = [p, u64, p]
+        L.psacak32.argtypes = [p, u64, p]
+        L.psacak8_ctx.argtypes = [p, p, u64, p, p]
+        L.psacak32_ctx.argtypes = [p, p, u64, p, p]
+        L.psacak8_dev.argtypes = [p, p, u64, p, p, p]
+        L.psacak32_dev.argtypes = [p, p, u64, p, p, p]
+        L.psacak8_batch.argtypes = [p, p, p, u32, p, p]
+        L.psacak_get_trace.argtypes = [p, p, u32, ctypes.POINTER(u32)]
+        L.psacak_check_sa8_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
+        L.psacak_check_sa32_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
+        L.psacak_kernel_launches.argtypes = [p]
+        L.psacak_kernel_launches.restype = u64
+        for name in ("psacak8", "psacak32", "psacak8_ctx", "psacak32_ctx", "psacak8_dev", "psacak32_dev",
+                     "psacak8_batch", "psacak_get_trace", "psacak_check_sa8_dev", "psacak_check_sa32_dev",
+                     "psacak_ctx_create", "psacak_ctx_destroy"):
+            getattr(L, name).restype = i32
+        _lib = L
+        return L
+
+
+def _raise(rc):
+    if rc != PSACAK_OK:
+        msg = lib().psacak_last_error_string()
+        raise PsacakError(rc, msg.decode() if msg else "")
+
+
+def _as_u8(text):
+    if isinstance(text, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bytes(text), dtype=np.uint8)
+    a = np.ascontiguousarray(text)
+    if a.dtype != np.uint8:
+        raise TypeError("psacak expects bytes or a uint8 array, got %s" % a.dtype)
+    return a.reshape(-1)
+
+
+def _vp(a):
+    return ctypes.c_void_p(a.ctypes.data) if a.size else ctypes.c_void_p(0)
+
+
+class Context:
+    """A builder context on one CUDA device (psacak_ctx).  It owns a stream,
+    a cached device workspace and the trace of its last build."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        _raise(lib().psacak_ctx_create(int(device), ctypes.byref(h)))
+        self._h = h
+        self.device = int(device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().psacak_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- host-pointer builds -------------------------------------------------
+    def psacak(self, text, schedule=None):
+        t = _as_u8(text)
+        if t.size >= 0xFFFFFFFF:
+            raise ValueError("text length must be below 2**32 - 1")
+        suf = np.empty(t.size, dtype=np.uint32)
+        _raise(lib().psacak8_ctx(self._h, _vp(t), t.size, _vp(suf), _sched_ptr(schedule)))
+        return suf
+
+    def psacak32(self, symbols, schedule=None):
+        t = np.ascontiguousarray(symbols, dtype=np.uint32).reshape(-1)
+        if t.size > 0x7FFFFFFF:
+            raise ValueError("symbol string length must be at most 2**31 - 1")
+        suf = np.empty(t.size, dtype=np.uint32)
+        _raise(lib().psacak32_ctx(self._h, _vp(t), t.size, _vp(suf), _sched_ptr(schedule)))
+        return suf
+
+    def psacak_batch(self, texts, schedule=None):
+        arrs = [_as_u8(t) for t in texts]
+        sas = [np.empty(a.size, dtype=np.uint32) for a in arrs]
+        n = len(arrs)
+        tp = (ctypes.c_void_p * n)(*[a.ctypes.data if a.size else 0 for a in arrs])
+        sp = (ctypes.c_void_p * n)(*[s.ctypes.data if s.size else 0 for s in sas])
+        lens = (ctypes.c_uint64 * n)(*[a.size for a in arrs])
+        _raise(lib().psacak8_batch(self._h, tp, lens, n, sp, _sched_ptr(schedule)))
+        return sas
+
+    # -- device-pointer builds (integer pointers, e.g. torch data_ptr()) ----
+    def psacak8_dev(self, d_text, n, d_sa, stream=0, schedule=None):
+        _raise(lib().psacak8_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                 ctypes.c_void_p(stream), _sched_ptr(schedule)))
+
+    def psacak32_dev(self, d_text, n, d_sa, stream=0, schedule=None):
+        _raise(lib().psacak32_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                  ctypes.c_void_p(stream), _sched_ptr(schedule)))
+
+    def check_sa8_dev(self, d_text, n, d_sa, stream=0):
+        ok = ctypes.c_int(0)
+        _raise(lib().psacak_check_sa8_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                          ctypes.byref(ok), ctypes.c_void_p(stream)))
+        return bool(ok.value)
+
+    def check_sa32_dev(self, d_text, n, d_sa, stream=0):
+        ok = ctypes.c_int(0)
+        _raise(lib().psacak_check_sa32_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                           ctypes.byref(ok), ctypes.c_void_p(stream)))
+        return bool(ok.value)
+
+    def trace(self):
+        buf = (LevelInfo * 128)()
+        cnt = ctypes.c_uint32(0)
+        _raise(lib().psacak_get_trace(self._h, buf, 128, ctypes.byref(cnt)))
+        return [dict(level=l.level, width=l.width, m=l.m, n_lms=l.n_lms, k=l.k, hash=l.hash)
+                for l in buf[:min(cnt.value, 128)]]
+
+    def kernel_launches(self):
+        return int(lib().psacak_kernel_launches(self._h))
+
+
+def _sched_ptr(schedule):
+    if schedule is None:
+        return None
+    if isinstance(schedule, dict):
+        s = Schedule()
+        for k, v in schedule.items():
+            setattr(s, k, int(v))
+        schedule = s
+    return ctypes.byref(schedule)
+
+
+_default = threading.local()
+
+
+def _ctx():
+    c = getattr(_default, "ctx", None)
+    if c is None:
+        c = Context(0)
+        _default.ctx = c
+    return c
+
+
+def psacak(text):
+    """Suffix array of a byte string (src/lib.rs:64), sentinel excluded."""
+    return _ctx().psacak(text)
+
+
+def psacak_inplace(text, suf):
+    """Writes the suffix array of `text` into suf[:len(text)] (src/lib.rs:77)."""
+    t = _as_u8(text)
+    if not isinstance(suf, np.ndarray) or suf.dtype != np.uint32:
+        raise TypeError("suf must be a numpy uint32 array")
+    if t.size > suf.size:
+        raise ValueError("the suffix array is shorter than the text")
+    if t.size >= 0xFFFFFFFF:
+        raise ValueError("text length must be below 2**32 - 1")
+    out = _ctx().psacak(t)
+    suf[:t.size] = out
+
+
+def psacak32(symbols):
+    """Suffix array of an integer-alphabet string (uint32 symbols)."""
+    return _ctx().psacak32(symbols)

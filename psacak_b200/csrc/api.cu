@@ -1,0 +1,620 @@
+// api.cu -- level recursion (the reference's psacak8 / psacak32 drivers) and
+// the C ABI of include/psacak_b200.h.
+#include <stdio.h>
+#include <string.h>
+
+#include <memory>
+
+#include "ctx.cuh"
+#include "induce.cuh"
+
+namespace psk {
+
+const char *last_error();
+void clear_error();
+
+// ---------------------------------------------------------------------------
+// Small kernels used by the driver.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// Order-dependent hash of a u32 array: sum of mix64((i << 32) ^ v[i]).
+__global__ void k_hash_u32(const uint32_t *__restrict__ v, uint64_t n, unsigned long long *out) {
+    __shared__ unsigned long long sm[32];
+    unsigned long long acc = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        acc += mix64((i << 32) ^ (uint64_t)v[i]);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL_MASK, acc, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < blockDim.x / 32 ? sm[threadIdx.x] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL_MASK, acc, o);
+        if (threadIdx.x == 0) atomicAdd(out, acc);
+    }
+}
+
+// S-type counts of translated buckets: scnt[text[j]] += 1 for S positions.
+__global__ void k_count_s(const uint32_t *__restrict__ text, uint64_t n, const uint32_t *__restrict__ types,
+                          uint32_t *scnt) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+        if (bm_get(types, j)) atomicAdd(&scnt[text[j]], 1u);
+}
+
+struct SortedLmsPred {
+    const uint32_t *sa;
+    const uint32_t *lms;
+    uint64_t n;
+    uint32_t *err;
+    __device__ __forceinline__ bool operator()(uint64_t i) const {
+        uint32_t x = sa[i];
+        if (x >= n) {
+            dev_fail(err, DEVERR_RANGE);
+            return false;
+        }
+        return bm_get(lms, x);
+    }
+};
+struct SortedLmsEmit {
+    const uint32_t *sa;
+    uint32_t *out;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t slot) const { out[slot] = sa[i]; }
+};
+
+static inline uint32_t grid_for(uint64_t n, uint32_t cap = 16384) {
+    uint64_t g = ceil_div(n ? n : 1, 256);
+    return (uint32_t)(g < cap ? g : cap);
+}
+
+static status_t hash_device(Ctx &ctx, const uint32_t *v, uint64_t n, uint64_t *out) {
+    unsigned long long *d = (unsigned long long *)(ctx.d_scalars + 32);
+    PSK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx.stream));
+    k_hash_u32<<<grid_for(n, 2048), 256, 0, ctx.stream>>>(v, n, d);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    uint32_t h[2];
+    PSK_TRY(ctx.read_u32((const uint32_t *)d, h, 2));
+    *out = ((uint64_t)h[1] << 32) | h[0];
+    return PSACAK_OK;
+}
+
+static void trace_push(Ctx &ctx, uint32_t level, uint32_t width, uint64_t m, uint64_t n1, uint64_t k, uint64_t hash) {
+    psacak_level_info li;
+    li.level = level;
+    li.width = width;
+    li.m = m;
+    li.n_lms = n1;
+    li.k = k;
+    li.hash = hash;
+    ctx.trace.push_back(li);
+}
+
+static int engine_for(const Ctx &ctx, uint32_t level, bool bytes) {
+    uint32_t e = level == 0 ? ctx.sched.engine : ctx.sched.inner_engine;
+    if (e == PSACAK_ENGINE_BUCKET && !bytes) e = PSACAK_ENGINE_DOUBLING;
+    if (e == PSACAK_ENGINE_AUTO) e = PSACAK_ENGINE_DOUBLING;
+    return (int)e;
+}
+
+// ---------------------------------------------------------------------------
+// One recursion level (the reference's psacak8, src/psacak8.rs:19-53, and
+// psacak32, src/psacak32.rs:24-56): sort the LMS substrings by an induced
+// sort, name them, recurse on the reduced string (or invert it directly when
+// all names are unique), map the reduced SA back to LMS positions and run
+// the final induced sort.
+// ---------------------------------------------------------------------------
+template <class C>
+status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t level) {
+    cudaStream_t s = ctx.stream;
+    const uint32_t width = sizeof(C);
+    if (n <= 3) {
+        PSK_TRY(tiny_sa(text, n, sa, s));
+        trace_push(ctx, level, width, n, 0, 0, 0);
+        return PSACAK_OK;
+    }
+    const bool bytes = sizeof(C) == 1;
+    const uint64_t nwords = ceil_div(n, 32);
+    const uint64_t ntiles = ceil_div(n, TYPE_TILE);
+    DBuf<uint32_t> types, lms, wcnt, pref, tscratch;
+    PSK_TRY(types.init(ctx, nwords + 1));
+    PSK_TRY(lms.init(ctx, nwords + 1));
+    PSK_TRY(wcnt.init(ctx, nwords + 1));
+    PSK_TRY(pref.init(ctx, nwords + 1));
+    PSK_TRY(tscratch.init(ctx, 2 * ntiles + 1024));
+    DBuf<ByteHist> hist;
+    DBuf<ByteGeom> dgeom;
+    if (bytes) {
+        PSK_TRY(hist.init(ctx, 1));
+        PSK_TRY(dgeom.init(ctx, 1));
+    }
+    PSK_TRY(type_text<C>(text, n, types, lms, wcnt, bytes ? hist.get() : nullptr, tscratch, ctx.scan_ctas, s));
+    tscratch.reset();
+    PSK_TRY(lms_prefix(wcnt, nwords, pref, ctx.d_partial, ctx.d_scalars, ctx.scan_ctas, s));
+    wcnt.reset();
+    uint32_t n1u = 0;
+    PSK_TRY(ctx.read_u32(ctx.d_scalars, &n1u));
+    const uint64_t n1 = n1u;
+
+    ByteGeom hg;
+    Geom<C> geom;
+    DBuf<uint32_t> scnt, cursor;
+    if constexpr (sizeof(C) == 1) {
+        ByteHist hh;
+        PSK_CUDA(cudaMemcpyAsync(&hh, hist.get(), sizeof(ByteHist), cudaMemcpyDeviceToHost, s));
+        PSK_TRY(ctx.sync());
+        uint32_t acc = 0, lacc = 0;
+        for (int c = 0; c < 256; c++) {
+            hg.head[c] = acc;
+            acc += hh.count[c];
+            hg.tail[c] = acc;
+            hg.lcount[c] = hh.lcount[c];
+            hg.scount[c] = hh.count[c] - hh.lcount[c];
+            hg.lmscount[c] = hh.lmscount[c];
+            hg.lmsstart[c] = lacc;
+            lacc += hh.lmscount[c];
+        }
+        if (acc != n || lacc != n1)
+            return set_error(PSACAK_EINTERNAL, "level histogram does not add up (%u/%llu, %u/%llu)", acc,
+                             (unsigned long long)n, lacc, (unsigned long long)n1);
+        PSK_CUDA(cudaMemcpyAsync(dgeom.get(), &hg, sizeof(ByteGeom), cudaMemcpyHostToDevice, s));
+        geom.g = dgeom.get();
+        PSK_TRY(cursor.init(ctx, 256));
+        PSK_CUDA(cudaMemsetAsync(cursor.get(), 0, 256 * sizeof(uint32_t), s));
+    } else {
+        PSK_TRY(scnt.init(ctx, n));
+        PSK_CUDA(cudaMemsetAsync(scnt.get(), 0, n * sizeof(uint32_t), s));
+        k_count_s<<<grid_for(n), 256, 0, s>>>(text, n, types, scnt);
+        PSK_KCOUNT();
+        PSK_LAUNCH_CHECK();
+        geom.scnt = scnt.get();
+        PSK_TRY(cursor.init(ctx, n));
+        PSK_CUDA(cudaMemsetAsync(cursor.get(), 0, n * sizeof(uint32_t), s));
+    }
+    const int engine = engine_for(ctx, level, bytes);
+
+    // Stage 1: sort the LMS substrings.
+    if constexpr (sizeof(C) == 1) {
+        if (engine == PSACAK_ENGINE_BUCKET)
+            PSK_TRY(induce_bucket8(ctx, text, n, types, hg, dgeom.get(), INDUCE_LMS_SUBSTRINGS, nullptr, n1, sa, s));
+        else
+            PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_LMS_SUBSTRINGS, nullptr, n1, cursor,
+                                       sa, s));
+    } else {
+        PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_LMS_SUBSTRINGS, nullptr, n1, cursor, sa,
+                                   s));
+    }
+    cursor.reset();
+
+    // Stage 2: name them and build the reduced string.
+    DBuf<uint32_t> sorted, red, heads, flags, sa1;
+    uint32_t k = 0;
+    PSK_TRY(sorted.init(ctx, n1));
+    if (n1 > 0) {
+        PSK_TRY(compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_partial, ctx.d_scalars + 1,
+                        ctx.scan_ctas, s));
+        uint32_t got = 0;
+        PSK_TRY(ctx.read_u32(ctx.d_scalars + 1, &got));
+        if (got != n1)
+            return set_error(PSACAK_EINTERNAL, "level %u: %u LMS after the induced sort, expected %llu", level, got,
+                             (unsigned long long)n1);
+        PSK_TRY(red.init(ctx, n1));
+        PSK_TRY(heads.init(ctx, n1 + 1));
+        PSK_TRY(flags.init(ctx, n1));
+        PSK_TRY(name_lms<C>(text, n, lms, pref, sorted, n1, red, heads, flags, ctx.d_partial, ctx.d_scalars + 2,
+                            ctx.scan_ctas, s));
+        PSK_TRY(ctx.read_u32(ctx.d_scalars + 2, &k));
+    }
+    sorted.reset();
+    flags.reset();
+    PSK_TRY(sa1.init(ctx, n1));
+    if (n1 > 0) {
+        if (k < n1) {
+            {
+                const uint64_t w1 = ceil_div(n1, 32);
+                DBuf<uint32_t> t1, l1, c1, sc1;
+                PSK_TRY(t1.init(ctx, w1 + 1));
+                PSK_TRY(l1.init(ctx, w1 + 1));
+                PSK_TRY(c1.init(ctx, w1 + 1));
+                PSK_TRY(sc1.init(ctx, 2 * ceil_div(n1, TYPE_TILE) + 1024));
+                PSK_TRY(type_text<uint32_t>(red, n1, t1, l1, c1, nullptr, sc1, ctx.scan_ctas, s));
+                PSK_TRY(translate_names(red, n1, t1, heads, ctx.d_err, s));
+            }
+            heads.reset();
+            uint64_t hsh = 0;
+            PSK_TRY(hash_device(ctx, red, n1, &hsh));
+            trace_push(ctx, level, width, n, n1, k, hsh);
+            PSK_TRY(build_level<uint32_t>(ctx, red, n1, sa1, level + 1));
+        } else {
+            heads.reset();
+            trace_push(ctx, level, width, n, n1, k, 0);
+            PSK_TRY(direct_inverse(red, n1, sa1, ctx.d_err, s));
+        }
+        // red is free again; reuse it as the position list of the permutation.
+        PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
+    } else {
+        trace_push(ctx, level, width, n, 0, 0, 0);
+    }
+    red.reset();
+
+    // Stage 3: induce the whole suffix array from the sorted LMS suffixes.
+    if constexpr (sizeof(C) == 1) {
+        if (engine == PSACAK_ENGINE_BUCKET)
+            return induce_bucket8(ctx, text, n, types, hg, dgeom.get(), INDUCE_FINAL, sa1, n1, sa, s);
+        return induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
+    } else {
+        return induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// translate_sample on the device (src/psacak32.rs:912-943): the distinct
+// symbols in order give buckets; an L-type symbol becomes its bucket head
+// (count of smaller symbols), an S-type one its bucket tail - 1.
+// ---------------------------------------------------------------------------
+__global__ void k_iota(uint32_t *v, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        v[i] = (uint32_t)i;
+}
+__global__ void k_copy_u32(const uint32_t *a, uint32_t *b, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+struct HeadLoad {
+    const uint32_t *vals;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const {
+        return (i == 0 || vals[i] != vals[i - 1]) ? (uint32_t)(i + 1) : 0u;
+    }
+};
+struct HeadStore {
+    uint32_t *head;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t v) const {
+        head[i] = (excl > v ? excl : v) - 1;
+    }
+};
+struct TailLoad {  // reversed index r = n - 1 - i; marks the last item of a group
+    const uint32_t *vals;
+    uint64_t n;
+    __device__ __forceinline__ uint32_t operator()(uint64_t r) const {
+        uint64_t i = n - 1 - r;
+        return (i + 1 == n || vals[i + 1] != vals[i]) ? (uint32_t)(r + 1) : 0u;
+    }
+};
+struct TailStore {
+    const uint32_t *vals, *pos, *head, *types;
+    uint64_t n;
+    uint32_t *out;
+    __device__ __forceinline__ void operator()(uint64_t r, uint32_t excl, uint32_t v) const {
+        uint32_t inc = excl > v ? excl : v;
+        uint64_t i = n - 1 - r;
+        uint32_t tail = (uint32_t)(n - inc + 1);  // one past the last index of the group
+        uint32_t p = pos[i];
+        out[p] = bm_get(types, p) ? tail - 1 : head[i];
+    }
+};
+struct DistinctLoad {
+    const uint32_t *vals;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const {
+        return (i == 0 || vals[i] != vals[i - 1]) ? 1u : 0u;
+    }
+};
+struct NoStore {
+    __device__ __forceinline__ void operator()(uint64_t, uint32_t, uint32_t) const {}
+};
+
+status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa) {
+    cudaStream_t s = ctx.stream;
+    if (n == 0) return PSACAK_OK;
+    DBuf<uint32_t> k0, v0, k1, v1;
+    PSK_TRY(k0.init(ctx, n));
+    PSK_TRY(v0.init(ctx, n));
+    PSK_TRY(k1.init(ctx, n));
+    PSK_TRY(v1.init(ctx, n));
+    k_copy_u32<<<grid_for(n), 256, 0, s>>>(text, k0, n);
+    PSK_KCOUNT();
+    k_iota<<<grid_for(n), 256, 0, s>>>(v0, n);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    int in1 = 0;
+    PSK_TRY((radix_sort_pairs<uint32_t, uint32_t>(k0, v0, k1, v1, n, 0, 32, ctx.d_hist, &in1, ctx.radix_ctas, s)));
+    const uint32_t *vals = in1 ? k1.get() : k0.get();
+    const uint32_t *pos = in1 ? v1.get() : v0.get();
+    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(DistinctLoad{vals}, NoStore{}, n, ctx.d_partial, ctx.d_scalars + 3,
+                                                   OpSum<uint32_t>(), ctx.scan_ctas, s)));
+    uint32_t distinct = 0;
+    PSK_TRY(ctx.read_u32(ctx.d_scalars + 3, &distinct));
+    if (distinct >= n) {
+        // all symbols distinct: the suffix order is the symbol order.
+        k_copy_u32<<<grid_for(n), 256, 0, s>>>(pos, sa, n);
+        PSK_KCOUNT();
+        PSK_LAUNCH_CHECK();
+        trace_push(ctx, 0, 4, n, 0, 0, 0);
+        return PSACAK_OK;
+    }
+    const uint64_t nwords = ceil_div(n, 32);
+    DBuf<uint32_t> types, lms, wcnt, tscratch, head, t2;
+    PSK_TRY(types.init(ctx, nwords + 1));
+    PSK_TRY(lms.init(ctx, nwords + 1));
+    PSK_TRY(wcnt.init(ctx, nwords + 1));
+    PSK_TRY(tscratch.init(ctx, 2 * ceil_div(n, TYPE_TILE) + 1024));
+    PSK_TRY(type_text<uint32_t>(text, n, types, lms, wcnt, nullptr, tscratch, ctx.scan_ctas, s));
+    PSK_TRY(head.init(ctx, n));
+    PSK_TRY(t2.init(ctx, n));
+    PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(HeadLoad{vals}, HeadStore{head}, n, ctx.d_partial,
+                                                   (uint32_t *)nullptr, OpMax<uint32_t>(), ctx.scan_ctas, s)));
+    PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(TailLoad{vals, n}, TailStore{vals, pos, head, types, n, t2}, n,
+                                                   ctx.d_partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
+                                                   ctx.scan_ctas, s)));
+    types.reset();
+    lms.reset();
+    wcnt.reset();
+    tscratch.reset();
+    head.reset();
+    k0.reset();
+    v0.reset();
+    k1.reset();
+    v1.reset();
+    return build_level<uint32_t>(ctx, t2, n, sa, 0);
+}
+
+status_t ctx_init(Ctx &c, int device) {
+    PSK_CUDA(cudaSetDevice(device));
+    c.dev.id = device;
+    cudaDeviceProp prop;
+    PSK_CUDA(cudaGetDeviceProperties(&prop, device));
+    c.dev.num_sms = prop.multiProcessorCount;
+    c.dev.smem_optin = prop.sharedMemPerBlockOptin;
+    PSK_CUDA(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
+    c.stream = c.own_stream;
+    PSK_CUDA(cudaDeviceGetDefaultMemPool(&c.pool, device));
+    uint64_t thresh = UINT64_MAX;
+    PSK_CUDA(cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+    PSK_CUDA(cudaMallocHost(&c.h_pinned, 4096));
+    PSK_CUDA(cudaMalloc(&c.d_partial, MAX_CHUNKS * 4 * sizeof(uint32_t)));
+    PSK_CUDA(cudaMalloc(&c.d_hist, 256 * RADIX_MAX_CTAS * sizeof(uint32_t)));
+    PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
+    PSK_CUDA(cudaMalloc(&c.d_err, sizeof(uint32_t)));
+    PSK_CUDA(cudaMemset(c.d_err, 0, sizeof(uint32_t)));
+    c.scan_ctas = 4 * (uint32_t)c.dev.num_sms;
+    c.radix_ctas = 4 * (uint32_t)c.dev.num_sms;
+    if (c.scan_ctas > MAX_CHUNKS) c.scan_ctas = MAX_CHUNKS;
+    if (c.radix_ctas > RADIX_MAX_CTAS) c.radix_ctas = RADIX_MAX_CTAS;
+    return PSACAK_OK;
+}
+
+void ctx_free(Ctx &c) {
+    if (c.h_pinned) cudaFreeHost(c.h_pinned);
+    if (c.d_partial) cudaFree(c.d_partial);
+    if (c.d_hist) cudaFree(c.d_hist);
+    if (c.d_scalars) cudaFree(c.d_scalars);
+    if (c.d_err) cudaFree(c.d_err);
+    if (c.own_stream) cudaStreamDestroy(c.own_stream);
+    c.h_pinned = nullptr;
+}
+
+static void apply_schedule(Ctx &c, const psacak_schedule *sched) {
+    psacak_schedule d{};
+    if (sched) d = *sched;
+    c.sched = d;
+    uint32_t per = d.radix_ctas_per_sm ? d.radix_ctas_per_sm : 4;
+    c.radix_ctas = per * (uint32_t)c.dev.num_sms;
+    if (c.radix_ctas > RADIX_MAX_CTAS) c.radix_ctas = RADIX_MAX_CTAS;
+}
+
+// Common body of the device-pointer entry points.
+template <class C>
+status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream_t stream,
+                 const psacak_schedule *sched) {
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = stream ? stream : c.own_stream;
+    apply_schedule(c, sched);
+    c.trace.clear();
+    status_t st;
+    if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, n, d_sa, 0);
+    else st = build_psacak32(c, d_text, n, d_sa);
+    if (st != PSACAK_OK) {
+        cudaStreamSynchronize(c.stream);
+        return st;
+    }
+    PSK_TRY(c.sync());
+    PSK_TRY(c.check_device_error());
+    return PSACAK_OK;
+}
+
+template <class C>
+status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_schedule *sched) {
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = c.own_stream;
+    DBuf<C> dt;
+    DBuf<uint32_t> ds;
+    PSK_TRY(dt.init(c, n));
+    PSK_TRY(ds.init(c, n));
+    if (n) PSK_CUDA(cudaMemcpyAsync(dt.get(), text, n * sizeof(C), cudaMemcpyHostToDevice, c.stream));
+    PSK_TRY(run_dev<C>(c, dt.get(), n, ds.get(), c.own_stream, sched));
+    if (n) PSK_CUDA(cudaMemcpyAsync(sa, ds.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+    dt.reset();
+    ds.reset();
+    PSK_TRY(c.sync());
+    return PSACAK_OK;
+}
+
+}  // namespace psk
+
+using namespace psk;
+
+static thread_local psacak_ctx *t_default_ctx = nullptr;
+
+static int default_ctx(psacak_ctx **out) {
+    if (!t_default_ctx) {
+        int rc = psacak_ctx_create(0, &t_default_ctx);
+        if (rc != PSACAK_OK) return rc;
+    }
+    *out = t_default_ctx;
+    return PSACAK_OK;
+}
+
+extern "C" {
+
+const char *psacak_version(void) { return "0.1.0"; }
+
+const char *psacak_last_error_string(void) { return last_error(); }
+
+int psacak_ctx_create(int device, psacak_ctx **out) {
+    clear_error();
+    if (!out) return set_error(PSACAK_EINVAL, "psacak_ctx_create: null output pointer");
+    std::unique_ptr<psacak_ctx> c(new (std::nothrow) psacak_ctx());
+    if (!c) return set_error(PSACAK_ENOMEM, "psacak_ctx_create: out of host memory");
+    int rc = ctx_init(c->c, device);
+    if (rc != PSACAK_OK) {
+        ctx_free(c->c);
+        return rc;
+    }
+    *out = c.release();
+    return PSACAK_OK;
+}
+
+int psacak_ctx_destroy(psacak_ctx *ctx) {
+    if (!ctx) return PSACAK_OK;
+    if (t_default_ctx == ctx) t_default_ctx = nullptr;
+    {
+        std::lock_guard<std::mutex> g(ctx->c.mu);
+        cudaSetDevice(ctx->c.dev.id);
+        cudaStreamSynchronize(ctx->c.own_stream);
+        ctx_free(ctx->c);
+    }
+    delete ctx;
+    return PSACAK_OK;
+}
+
+static int check_args8(const void *text, uint64_t n, const void *sa) {
+    if (n > 0 && (!text || !sa)) return set_error(PSACAK_EINVAL, "null text or suffix-array pointer");
+    if (n >= 0xFFFFFFFFull) return set_error(PSACAK_EINVAL, "text length %llu is not below 2^32-1", (unsigned long long)n);
+    return PSACAK_OK;
+}
+static int check_args32(const void *text, uint64_t n, const void *sa) {
+    if (n > 0 && (!text || !sa)) return set_error(PSACAK_EINVAL, "null text or suffix-array pointer");
+    if (n > 0x7FFFFFFFull) return set_error(PSACAK_EINVAL, "text length %llu exceeds 2^31-1", (unsigned long long)n);
+    return PSACAK_OK;
+}
+
+int psacak8_ctx(psacak_ctx *ctx, const uint8_t *text, uint64_t n, uint32_t *sa, const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    int rc = check_args8(text, n, sa);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    return run_host<uint8_t>(ctx->c, text, n, sa, sched);
+}
+
+int psacak32_ctx(psacak_ctx *ctx, const uint32_t *text, uint64_t n, uint32_t *sa, const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    int rc = check_args32(text, n, sa);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    return run_host<uint32_t>(ctx->c, text, n, sa, sched);
+}
+
+int psacak8(const uint8_t *text, uint64_t n, uint32_t *sa) {
+    clear_error();
+    int rc = check_args8(text, n, sa);
+    if (rc) return rc;
+    psacak_ctx *c = nullptr;
+    rc = default_ctx(&c);
+    if (rc) return rc;
+    return psacak8_ctx(c, text, n, sa, nullptr);
+}
+
+int psacak32(const uint32_t *text, uint64_t n, uint32_t *sa) {
+    clear_error();
+    int rc = check_args32(text, n, sa);
+    if (rc) return rc;
+    psacak_ctx *c = nullptr;
+    rc = default_ctx(&c);
+    if (rc) return rc;
+    return psacak32_ctx(c, text, n, sa, nullptr);
+}
+
+int psacak8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, uint32_t *d_sa, void *stream,
+                const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    int rc = check_args8(d_text, n, d_sa);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    return run_dev<uint8_t>(ctx->c, d_text, n, d_sa, (cudaStream_t)stream, sched);
+}
+
+int psacak32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, uint32_t *d_sa, void *stream,
+                 const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    int rc = check_args32(d_text, n, d_sa);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    return run_dev<uint32_t>(ctx->c, d_text, n, d_sa, (cudaStream_t)stream, sched);
+}
+
+int psacak_get_trace(psacak_ctx *ctx, psacak_level_info *out, uint32_t cap, uint32_t *count) {
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    uint32_t n = (uint32_t)ctx->c.trace.size();
+    for (uint32_t i = 0; i < n && i < cap && out; i++) out[i] = ctx->c.trace[i];
+    if (count) *count = n;
+    return PSACAK_OK;
+}
+
+}  // extern "C"
+
+template <class C>
+static int check_dev(psacak_ctx *ctx, const C *d_text, uint64_t n, const uint32_t *d_sa, int *ok, void *stream) {
+    clear_error();
+    if (!ctx || !ok) return set_error(PSACAK_EINVAL, "null context or result pointer");
+    if (n > 0 && (!d_text || !d_sa)) return set_error(PSACAK_EINVAL, "null text or suffix-array pointer");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = stream ? (cudaStream_t)stream : c.own_stream;
+    DBuf<uint32_t> isa;
+    PSK_TRY(isa.init(c, n));
+    PSK_TRY(check_sa<C>(d_text, n, d_sa, isa, c.d_scalars + 40, c.stream));
+    uint32_t bad = 0;
+    PSK_TRY(c.read_u32(c.d_scalars + 40, &bad));
+    *ok = bad == 0;
+    return PSACAK_OK;
+}
+
+extern "C" {
+
+int psacak_check_sa8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, const uint32_t *d_sa, int *ok,
+                         void *stream) {
+    return check_dev<uint8_t>(ctx, d_text, n, d_sa, ok, stream);
+}
+
+int psacak_check_sa32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, const uint32_t *d_sa, int *ok,
+                          void *stream) {
+    return check_dev<uint32_t>(ctx, d_text, n, d_sa, ok, stream);
+}
+
+uint64_t psacak_kernel_launches(psacak_ctx *ctx) {
+    (void)ctx;
+    return g_kernel_launches.load();
+}
+
+int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *lens, uint32_t n_texts,
+                  uint32_t *const *sas, const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    if (n_texts > 0 && (!texts || !lens || !sas)) return set_error(PSACAK_EINVAL, "null batch arrays");
+    for (uint32_t i = 0; i < n_texts; i++) {
+        int rc = psacak8_ctx(ctx, texts[i], lens[i], sas[i], sched);
+        if (rc) return rc;
+    }
+    return PSACAK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// induce.cuh -- induced L-/S-scans of one level.
+#pragma once
+
+#include "level.cuh"
+
+namespace psk {
+
+struct Ctx;
+
+// Geometry of the buckets of a byte level (SA-position space), uploaded from
+// the host after the level histogram is read back.
+struct ByteGeom {
+    uint32_t head[256];    // first SA slot of bucket c
+    uint32_t tail[256];    // one past the last slot of bucket c
+    uint32_t lcount[256];  // L-type suffixes of bucket c
+    uint32_t scount[256];  // S-type suffixes of bucket c
+    uint32_t lmscount[256];
+    uint32_t lmsstart[256];  // first index of bucket c in the sorted LMS list
+};
+
+// Geometry of a translated integer level: every L-type symbol is its bucket
+// head and every S-type symbol is its bucket tail - 1 (the reference's
+// translate, src/naming.rs:263-274).  scnt[v] = S-type count of the bucket
+// whose tail - 1 is v.
+struct WordGeom {
+    const uint32_t *scnt;
+};
+
+template <class C> struct Geom;
+template <> struct Geom<uint8_t> {
+    const ByteGeom *g;
+    __device__ __forceinline__ uint32_t lgroup(uint8_t c) const { return g->head[c]; }
+    __device__ __forceinline__ uint32_t sgroup(uint8_t c) const { return g->tail[c] - g->scount[c]; }
+    __device__ __forceinline__ uint32_t tail(uint8_t c) const { return g->tail[c]; }
+    __device__ __forceinline__ uint32_t bucket(uint8_t c) const { return c; }
+};
+template <> struct Geom<uint32_t> {
+    const uint32_t *scnt;
+    __device__ __forceinline__ uint32_t lgroup(uint32_t v) const { return v; }
+    __device__ __forceinline__ uint32_t sgroup(uint32_t v) const { return v + 1 - scnt[v]; }
+    __device__ __forceinline__ uint32_t tail(uint32_t v) const { return v + 1; }
+    __device__ __forceinline__ uint32_t bucket(uint32_t v) const { return v; }
+};
+
+enum InduceMode { INDUCE_LMS_SUBSTRINGS = 0, INDUCE_FINAL = 1 };
+
+// Chain-doubling induced sort.  In INDUCE_LMS_SUBSTRINGS mode the LMS
+// positions start in arbitrary order at their bucket tails; in INDUCE_FINAL
+// mode `sorted_lms` (n1 entries, ascending suffix order) gives their order.
+// Writes every SA slot.  `cursor` is n (u32 levels) or 256 (byte levels)
+// zeroed uint32 used to place LMS positions in the first mode.
+template <class C>
+status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
+                         Geom<C> geom, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
+                         uint32_t *cursor, uint32_t *sa, cudaStream_t s);
+
+// Bucket-ordered induced sort of a byte level (the reference's induce scan
+// processed one bucket at a time): every bucket's L part is completed and
+// then scattered to the higher buckets in scan order; the S scan mirrors it.
+status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *types,
+                        const ByteGeom &hgeom, const ByteGeom *dgeom, InduceMode mode, const uint32_t *sorted_lms,
+                        uint64_t n1, uint32_t *sa, cudaStream_t s);
+
+}  // namespace psk

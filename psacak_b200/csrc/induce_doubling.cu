@@ -1,0 +1,252 @@
+// induce_doubling.cu -- the induced L-/S-scans of one level as chain doubling.
+//
+// The reference's scans (src/psacak8.rs:127-190, src/psacak32.rs:137-275)
+// place every L-type suffix j at the next free slot of bucket text[j] in the
+// order in which its successor j+1 is met by the left-to-right scan, and
+// every S-type suffix, right to left, in the order of its successor.  The
+// L part of a bucket is therefore sorted by the rank of j+1, which is itself
+// an L suffix sorted the same way, until the chain reaches an LMS position
+// whose slot is known before the scan starts (the "terminal").  In SA-slot
+// space every L-type character can stand for the head of its bucket and the
+// terminal for its exact slot; comparing these integer chains
+// lexicographically reproduces the scan's order (L before S inside a
+// bucket, buckets in character order).  The S scan is the mirror image with
+// S-type characters standing for the start of the S part and the L slots
+// found by the L scan as terminals.
+//
+// This file resolves those chains with rank doubling: every unresolved item
+// (group start g, position j) is keyed by (g, rank[j + h]) for h = 1, 2, 4,
+// ...; a round sorts the keys (LSD radix), splits groups where keys differ
+// and gives singleton groups their final slot.  Chains end at a terminal,
+// so the number of rounds is log2 of the longest L or S run, not of the
+// longest repeat.  Nothing here depends on the size of the alphabet.
+#include "ctx.cuh"
+#include "induce.cuh"
+
+namespace psk {
+
+struct Tri {
+    uint32_t g, s, k;
+};
+__device__ __forceinline__ Tri shfl_up_t(Tri v, int o) {
+    Tri r;
+    r.g = __shfl_up_sync(FULL_MASK, v.g, o);
+    r.s = __shfl_up_sync(FULL_MASK, v.s, o);
+    r.k = __shfl_up_sync(FULL_MASK, v.k, o);
+    return r;
+}
+struct OpTri {
+    __device__ __forceinline__ Tri operator()(Tri a, Tri b) const {
+        Tri r;
+        r.g = a.g > b.g ? a.g : b.g;
+        r.s = a.s > b.s ? a.s : b.s;
+        r.k = a.k + b.k;
+        return r;
+    }
+    __device__ __forceinline__ static Tri identity() { return Tri{0, 0, 0}; }
+};
+
+// ---- terminal slots of the LMS positions ---------------------------------
+
+// LMS-substring mode: LMS positions take distinct slots at the tail of their
+// bucket in arbitrary order (the reference's put_lmscharacters,
+// src/psacak8.rs:57-72 / src/psacak32.rs:60-99).
+template <class C>
+__global__ void k_place_lms_any(const C *__restrict__ text, uint64_t nwords, const uint32_t *__restrict__ lms,
+                                Geom<C> g, uint32_t *cursor, uint32_t *R) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t word = lms[w];
+        while (word) {
+            int b = __ffs(word) - 1;
+            word &= word - 1;
+            uint64_t p = (w << 5) + b;
+            C c = text[p];
+            uint32_t slot = atomicAdd(&cursor[g.bucket(c)], 1u);
+            R[p] = g.tail(c) - slot;  // slot tail-1-slot, plus one
+        }
+    }
+}
+
+// Final mode: the sorted LMS suffixes fill the tail of each bucket in order
+// (the reference's put_lmssuffixes, src/psacak8.rs:76-87 /
+// src/psacak32.rs:103-121).  `last` = index of the last list entry of the
+// same bucket, found by a max-scan over the reversed list.
+template <class C> struct LastLoad {
+    const C *text;
+    const uint32_t *sorted;
+    uint64_t n1;
+    Geom<C> g;
+    __device__ __forceinline__ uint32_t operator()(uint64_t r) const {
+        uint64_t i = n1 - 1 - r;
+        bool last = (i + 1 == n1) || g.bucket(text[sorted[i + 1]]) != g.bucket(text[sorted[i]]);
+        return last ? (uint32_t)(r + 1) : 0u;
+    }
+};
+template <class C> struct LastStore {
+    const C *text;
+    const uint32_t *sorted;
+    uint64_t n1;
+    Geom<C> g;
+    uint32_t *R;
+    __device__ __forceinline__ void operator()(uint64_t r, uint32_t excl, uint32_t v) const {
+        uint32_t inc = excl > v ? excl : v;
+        uint64_t i = n1 - 1 - r;
+        uint64_t last = n1 - inc;
+        uint32_t p = sorted[i];
+        R[p] = g.tail(text[p]) - (uint32_t)(last - i);
+    }
+};
+
+// ---- work list -----------------------------------------------------------
+
+template <class C, bool STYPE> struct WPred {
+    const uint32_t *types;
+    __device__ __forceinline__ bool operator()(uint64_t j) const { return bm_get(types, j) == STYPE; }
+};
+template <class C, bool STYPE> struct WEmit {
+    const C *text;
+    Geom<C> g;
+    uint32_t *Wg, *Wv, *R;
+    __device__ __forceinline__ void operator()(uint64_t j, uint32_t slot) const {
+        C c = text[j];
+        uint32_t grp = STYPE ? g.sgroup(c) : g.lgroup(c);
+        Wg[slot] = grp;
+        Wv[slot] = (uint32_t)j;
+        R[j] = grp + 1;
+    }
+};
+
+__global__ void k_keys(const uint32_t *__restrict__ Wg, const uint32_t *__restrict__ Wv, uint64_t cnt,
+                       const uint32_t *__restrict__ R, uint64_t n, uint64_t h, int KB, uint64_t *keys,
+                       uint32_t *vals, uint32_t *err) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t v = Wv[i];
+        uint64_t q = (uint64_t)v + h;
+        uint32_t r = 0;
+        if (q <= n) r = R[q];
+        else dev_fail(err, DEVERR_RANGE);
+        keys[i] = ((uint64_t)Wg[i] << KB) | r;
+        vals[i] = v;
+    }
+}
+
+struct RoundLoad {
+    const uint64_t *keys;
+    uint64_t cnt;
+    int KB;
+    __device__ __forceinline__ Tri operator()(uint64_t i) const {
+        uint64_t k = keys[i];
+        bool gb = true, sb = true, sbn = true;
+        if (i > 0) {
+            uint64_t kp = keys[i - 1];
+            gb = (kp >> KB) != (k >> KB);
+            sb = kp != k;
+        }
+        if (i + 1 < cnt) sbn = keys[i + 1] != k;
+        Tri t;
+        t.g = gb ? (uint32_t)(i + 1) : 0u;
+        t.s = sb ? (uint32_t)(i + 1) : 0u;
+        t.k = (sb && sbn) ? 0u : 1u;
+        return t;
+    }
+};
+struct RoundStore {
+    const uint64_t *keys;
+    const uint32_t *vals;
+    int KB;
+    uint32_t *R, *sa, *Wg, *Wv;
+    uint64_t n;
+    uint32_t *err;
+    __device__ __forceinline__ void operator()(uint64_t i, Tri excl, Tri v) const {
+        uint32_t gs = (excl.g > v.g ? excl.g : v.g) - 1;
+        uint32_t ss = (excl.s > v.s ? excl.s : v.s) - 1;
+        uint32_t g = (uint32_t)(keys[i] >> KB);
+        uint32_t newg = g + (ss - gs);
+        uint32_t val = vals[i];
+        if (newg >= n || val >= n) {
+            dev_fail(err, DEVERR_RANGE);
+            return;
+        }
+        R[val] = newg + 1;
+        if (v.k) {
+            Wg[excl.k] = newg;
+            Wv[excl.k] = val;
+        } else {
+            sa[newg] = val;
+        }
+    }
+};
+
+// One scan (L or S): resolves the chains of every item of the given type.
+template <class C, bool STYPE>
+static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, Geom<C> geom,
+                              uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0,
+                              uint64_t *k1, uint32_t *v1, cudaStream_t s) {
+    uint32_t *d_cnt = ctx.d_scalars;
+    PSK_TRY(compact(WPred<C, STYPE>{types}, WEmit<C, STYPE>{text, geom, Wg, Wv, R}, n, ctx.d_partial, d_cnt,
+                    ctx.scan_ctas, s));
+    uint32_t cnt = 0;
+    PSK_TRY(ctx.read_u32(d_cnt, &cnt));
+    const int KB = bitlen(n);
+    const int GB = bitlen(n - 1);
+    Tri *d_tri = (Tri *)(ctx.d_scalars + 4);
+    for (uint64_t h = 1; cnt > 0; h <<= 1) {
+        if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
+        uint64_t gblocks = ceil_div(cnt, 256);
+        k_keys<<<(uint32_t)(gblocks < 16384 ? gblocks : 16384), 256, 0, s>>>(Wg, Wv, cnt, R, n, h, KB, k0, v0,
+                                                                             ctx.d_err);
+        PSK_KCOUNT();
+        PSK_LAUNCH_CHECK();
+        int in1 = 0;
+        PSK_TRY((radix_sort_pairs<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, ctx.d_hist, &in1,
+                                                      ctx.radix_ctas, s)));
+        const uint64_t *ks = in1 ? k1 : k0;
+        const uint32_t *vs = in1 ? v1 : v0;
+        PSK_TRY((chunk_scan<Tri, OpTri>(RoundLoad{ks, cnt, KB}, RoundStore{ks, vs, KB, R, sa, Wg, Wv, n, ctx.d_err}, cnt,
+                                        (Tri *)ctx.d_partial, d_tri, OpTri(), ctx.scan_ctas, s)));
+        uint32_t tri[3];
+        PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 3));
+        cnt = tri[2];
+    }
+    return PSACAK_OK;
+}
+
+template <class C>
+status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
+                         Geom<C> geom, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1, uint32_t *cursor,
+                         uint32_t *sa, cudaStream_t s) {
+    DBuf<uint32_t> R, Wg, Wv, v0, v1;
+    DBuf<uint64_t> k0, k1;
+    PSK_TRY(R.init(ctx, n + 1));
+    PSK_TRY(Wg.init(ctx, n));
+    PSK_TRY(Wv.init(ctx, n));
+    PSK_TRY(v0.init(ctx, n));
+    PSK_TRY(v1.init(ctx, n));
+    PSK_TRY(k0.init(ctx, n));
+    PSK_TRY(k1.init(ctx, n));
+    PSK_CUDA(cudaMemsetAsync(R.get() + n, 0, sizeof(uint32_t), s));  // the sentinel ranks lowest
+    const uint64_t nwords = ceil_div(n, 32);
+    if (mode == INDUCE_LMS_SUBSTRINGS) {
+        uint64_t g = ceil_div(nwords, 256);
+        k_place_lms_any<C><<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(text, nwords, lms, geom, cursor, R);
+        PSK_KCOUNT();
+        PSK_LAUNCH_CHECK();
+    } else if (n1 > 0) {
+        PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{text, sorted_lms, n1, geom},
+                                                       LastStore<C>{text, sorted_lms, n1, geom, R}, n1,
+                                                       ctx.d_partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
+                                                       ctx.scan_ctas, s)));
+    }
+    PSK_TRY((doubling_scan<C, false>(ctx, text, n, types, geom, R, sa, Wg, Wv, k0, v0, k1, v1, s)));
+    PSK_TRY((doubling_scan<C, true>(ctx, text, n, types, geom, R, sa, Wg, Wv, k0, v0, k1, v1, s)));
+    return PSACAK_OK;
+}
+
+template status_t induce_doubling<uint8_t>(Ctx &, const uint8_t *, uint64_t, const uint32_t *, const uint32_t *,
+                                           Geom<uint8_t>, InduceMode, const uint32_t *, uint64_t, uint32_t *,
+                                           uint32_t *, cudaStream_t);
+template status_t induce_doubling<uint32_t>(Ctx &, const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
+                                            Geom<uint32_t>, InduceMode, const uint32_t *, uint64_t, uint32_t *,
+                                            uint32_t *, cudaStream_t);
+
+}  // namespace psk

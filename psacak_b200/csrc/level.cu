@@ -1,0 +1,467 @@
+// level.cu -- per-level kernels (typing, naming, translation, permutation).
+#include "level.cuh"
+
+namespace psk {
+
+// ---------------------------------------------------------------------------
+// L/S typing (the reference's foreach_typedchars, src/common.rs:43-68).
+//
+// Position i is S iff text[i] < text[i+1], L iff text[i] > text[i+1], and
+// takes the type of i+1 when the two are equal; n-1 is L.  So the type of i
+// is the type of the first "change point" q >= i (q = n-1 or text[q] !=
+// text[q+1]).  Each warp builds 32-position words with ballots, a block-wide
+// max-scan finds for every word the nearest change point to its right inside
+// the 8192-position tile, and a per-tile carry (computed by a chunked
+// max-scan over tiles) covers equal runs that cross tiles.
+// ---------------------------------------------------------------------------
+
+// Code of the first change point of each tile: 0 none, 1 L, 2 S.
+template <class C>
+__global__ void __launch_bounds__(TYPE_BLOCK) k_tile_first(const C *__restrict__ text, uint64_t n,
+                                                           uint64_t ntiles, uint32_t *code_out) {
+    __shared__ unsigned long long s_first;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint64_t start = tile * TYPE_TILE;
+        uint64_t end = start + TYPE_TILE < n ? start + TYPE_TILE : n;
+        if (threadIdx.x == 0) s_first = ~0ull;
+        __syncthreads();
+        uint32_t code = 0;
+        for (uint64_t base = start; base < end; base += TYPE_BLOCK) {
+            uint64_t p = base + threadIdx.x;
+            bool c = p < end && (p == n - 1 || text[p] != text[p + 1]);
+            if (c) atomicMin(&s_first, (unsigned long long)p);
+            if (__syncthreads_or(c)) {
+                uint64_t q = s_first;
+                uint32_t t = (q == n - 1) ? 0u : (text[q] < text[q + 1] ? 1u : 0u);
+                code = 1 + t;
+                break;
+            }
+        }
+        if (threadIdx.x == 0) code_out[tile] = code;
+        __syncthreads();
+    }
+}
+
+struct TileCarryLoad {
+    const uint32_t *code;
+    uint64_t T;
+    __device__ __forceinline__ uint32_t operator()(uint64_t r) const {
+        uint32_t c = code[T - 1 - r];
+        return c ? (uint32_t)(((r + 1) << 1) | (c - 1)) : 0u;
+    }
+};
+struct TileCarryStore {
+    uint32_t *carry;
+    uint64_t T;
+    __device__ __forceinline__ void operator()(uint64_t r, uint32_t excl, uint32_t) const {
+        carry[T - 1 - r] = excl ? (excl & 1u) : 0u;
+    }
+};
+
+template <class C, bool HIST>
+__global__ void __launch_bounds__(TYPE_BLOCK) k_type_main(const C *__restrict__ text, uint64_t n, uint64_t ntiles,
+                                                          const uint32_t *__restrict__ tile_carry,
+                                                          uint32_t *__restrict__ types, uint32_t *__restrict__ lms,
+                                                          uint32_t *__restrict__ lms_wcnt, ByteHist *ghist) {
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_hi[TYPE_BLOCK];
+    __shared__ uint32_t s_hist[HIST ? 3 * 256 : 1];
+    const int w = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwords = ceil_div(n, 32);
+    if (HIST)
+        for (int i = threadIdx.x; i < 3 * 256; i += TYPE_BLOCK) s_hist[i] = 0;
+
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t tstart = tile * TYPE_TILE;
+        uint32_t myC = 0, myD = 0;
+        uint32_t pk[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int it = 0; it < 32; it++) {
+            uint64_t p = tstart + (uint64_t)(w * 32 + it) * 32 + lane;
+            bool valid = p < n;
+            C a = valid ? text[p] : C(0);
+            C b = (p + 1 < n) ? text[p + 1] : C(0);
+            bool last = (p == n - 1);
+            bool c = valid && (last || a != b);
+            bool sd = valid && !last && a < b;
+            uint32_t cw = __ballot_sync(FULL_MASK, c);
+            uint32_t dw = __ballot_sync(FULL_MASK, sd);
+            if ((int)lane == it) {
+                myC = cw;
+                myD = dw;
+            }
+            if (HIST) pk[it >> 2] |= ((uint32_t)(uint8_t)a) << ((it & 3) * 8);
+        }
+        // nearest change point to the right of this word within the tile
+        const uint32_t r = TYPE_BLOCK - 1 - threadIdx.x;
+        uint32_t enc = 0;
+        if (myC) {
+            int lb = __ffs(myC) - 1;
+            enc = ((r + 1) << 1) | ((myD >> lb) & 1u);
+        }
+        uint32_t excl;
+        block_scan<uint32_t, OpMax<uint32_t>, TYPE_BLOCK>(enc, OpMax<uint32_t>(), s_scan, &excl, (uint32_t *)nullptr);
+        uint32_t cur = excl ? (excl & 1u) : tile_carry[tile];
+        uint32_t T = 0;
+#pragma unroll
+        for (int k = 31; k >= 0; k--) {
+            if ((myC >> k) & 1u) cur = (myD >> k) & 1u;
+            T |= cur << k;
+        }
+        const uint64_t wg = tile * TYPE_BLOCK + threadIdx.x;
+        const uint64_t p0 = wg * 32;
+        uint32_t vmask = 0;
+        if (p0 < n) vmask = (n - p0 >= 32) ? FULL_MASK : (uint32_t)((1ull << (n - p0)) - 1);
+        T &= vmask;
+        s_hi[threadIdx.x] = T >> 31;
+        __syncthreads();
+        uint32_t prevS;
+        if (threadIdx.x > 0) {
+            prevS = s_hi[threadIdx.x - 1];
+        } else if (p0 == 0 || p0 >= n) {
+            prevS = 1;  // position 0 is never LMS
+        } else {
+            C x = text[p0 - 1], y = text[p0];
+            prevS = (x != y) ? (x < y ? 1u : 0u) : (T & 1u);
+        }
+        uint32_t Lm = T & ~((T << 1) | prevS) & vmask;
+        if (wg < nwords) {
+            types[wg] = T;
+            lms[wg] = Lm;
+            lms_wcnt[wg] = __popc(Lm);
+        }
+        if (HIST) {
+#pragma unroll
+            for (int it = 0; it < 32; it++) {
+                uint32_t Tw = __shfl_sync(FULL_MASK, T, it);
+                uint32_t Lw = __shfl_sync(FULL_MASK, Lm, it);
+                uint64_t p = tstart + (uint64_t)(w * 32 + it) * 32 + lane;
+                bool valid = p < n;
+                uint32_t a = (pk[it >> 2] >> ((it & 3) * 8)) & 0xFFu;
+                uint32_t key = valid ? a : 256u;
+                uint32_t peers = __match_any_sync(FULL_MASK, key);
+                uint32_t lb = __ballot_sync(FULL_MASK, valid && !((Tw >> lane) & 1u));
+                uint32_t mb = __ballot_sync(FULL_MASK, valid && ((Lw >> lane) & 1u));
+                if (valid && (int)lane == __ffs(peers) - 1) {
+                    atomicAdd(&s_hist[a], __popc(peers));
+                    uint32_t nl = __popc(peers & lb), nm = __popc(peers & mb);
+                    if (nl) atomicAdd(&s_hist[256 + a], nl);
+                    if (nm) atomicAdd(&s_hist[512 + a], nm);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (HIST) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 256; i += TYPE_BLOCK) {
+            if (s_hist[i]) atomicAdd(&ghist->count[i], s_hist[i]);
+            if (s_hist[256 + i]) atomicAdd(&ghist->lcount[i], s_hist[256 + i]);
+            if (s_hist[512 + i]) atomicAdd(&ghist->lmscount[i], s_hist[512 + i]);
+        }
+    }
+}
+
+template <class C>
+status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, uint32_t *lms_wcnt,
+                   ByteHist *hist, uint32_t *scratch, uint32_t max_ctas, cudaStream_t s) {
+    if (n == 0) return PSACAK_OK;
+    uint64_t ntiles = ceil_div(n, TYPE_TILE);
+    uint32_t *code = scratch;
+    uint32_t *carry = scratch + ntiles;
+    uint32_t *partial = scratch + 2 * ntiles;
+    uint32_t grid = (uint32_t)(ntiles < max_ctas ? ntiles : max_ctas);
+    k_tile_first<C><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, code);
+    PSK_KCOUNT();
+    PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(TileCarryLoad{code, ntiles}, TileCarryStore{carry, ntiles},
+                                                   ntiles, partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
+                                                   max_ctas, s)));
+    if (hist) {
+        PSK_CUDA(cudaMemsetAsync(hist, 0, sizeof(ByteHist), s));
+        k_type_main<C, true><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, carry, types, lms, lms_wcnt, hist);
+    } else {
+        k_type_main<C, false><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, carry, types, lms, lms_wcnt, nullptr);
+    }
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
+template status_t type_text<uint8_t>(const uint8_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, ByteHist *,
+                                     uint32_t *, uint32_t, cudaStream_t);
+template status_t type_text<uint32_t>(const uint32_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, ByteHist *,
+                                      uint32_t *, uint32_t, cudaStream_t);
+
+struct PrefLoad {
+    const uint32_t *w;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return w[i]; }
+};
+struct PrefStore {
+    uint32_t *pref;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t) const { pref[i] = excl; }
+};
+
+__global__ void k_copy_total(const uint32_t *total, uint32_t *dst) { *dst = *total; }
+
+status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *partial,
+                    uint32_t *total, uint32_t max_ctas, cudaStream_t s) {
+    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(PrefLoad{lms_wcnt}, PrefStore{pref}, nwords, partial, total,
+                                                   OpSum<uint32_t>(), max_ctas, s)));
+    k_copy_total<<<1, 1, 0, s>>>(total, pref + nwords);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Naming (the reference's name_lmssubstrings, src/naming.rs:20-93, with the
+// equality of UintFingerprint::equals, src/naming.rs:388-408): two LMS
+// substrings are equal iff they have the same length up to and including the
+// next LMS position and the same characters; a substring that reaches the
+// end of the text contains the sentinel and equals nothing else.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t next_lms(const uint32_t *lms, uint64_t n, uint64_t p) {
+    uint64_t w = p >> 5;
+    uint32_t sh = (uint32_t)(p & 31);
+    uint32_t word = sh == 31 ? 0u : (lms[w] & (FULL_MASK << (sh + 1)));
+    const uint64_t nwords = ceil_div(n, 32);
+    while (!word) {
+        w++;
+        if (w >= nwords) return n;
+        word = lms[w];
+    }
+    return (w << 5) + (uint64_t)(__ffs(word) - 1);
+}
+
+template <class C>
+__device__ bool lms_equal(const C *text, uint64_t n, const uint32_t *lms, uint64_t a, uint64_t b) {
+    uint64_t ea = next_lms(lms, n, a), eb = next_lms(lms, n, b);
+    if (ea >= n || eb >= n) return false;
+    uint64_t la = ea - a, lb = eb - b;
+    if (la != lb) return false;
+    for (uint64_t k = 0; k <= la; k++)
+        if (text[a + k] != text[b + k]) return false;
+    return true;
+}
+
+template <class C>
+__global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint32_t *__restrict__ lms,
+                             const uint32_t *__restrict__ sorted, uint64_t n1, uint32_t *flags) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t f = 1;
+        if (i > 0) f = lms_equal(text, n, lms, sorted[i - 1], sorted[i]) ? 0u : 1u;
+        flags[i] = f;
+    }
+}
+
+struct NameLoad {
+    const uint32_t *flags;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return flags[i]; }
+};
+struct NameStore {
+    const uint32_t *sorted;
+    const uint32_t *lms;
+    const uint32_t *pref;
+    uint32_t *red;
+    uint32_t *heads;
+    uint64_t n1;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t v) const {
+        uint32_t name = excl + v - 1;
+        red[lms_rank(lms, pref, sorted[i])] = name;
+        if (v) heads[name] = (uint32_t)i;
+        if (i == n1 - 1) heads[name + 1] = (uint32_t)n1;
+    }
+};
+
+template <class C>
+status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t *lms_pref,
+                  const uint32_t *sorted, uint64_t n1, uint32_t *red, uint32_t *heads, uint32_t *flags,
+                  uint32_t *partial, uint32_t *k_out, uint32_t max_ctas, cudaStream_t s) {
+    if (n1 == 0) {
+        PSK_CUDA(cudaMemsetAsync(k_out, 0, sizeof(uint32_t), s));
+        return PSACAK_OK;
+    }
+    uint32_t grid = (uint32_t)(ceil_div(n1, 256) < (uint64_t)max_ctas * 4 ? ceil_div(n1, 256) : (uint64_t)max_ctas * 4);
+    k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lms, sorted, n1, flags);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return chunk_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags}, NameStore{sorted, lms, lms_pref, red, heads, n1},
+                                                 n1, partial, k_out, OpSum<uint32_t>(), max_ctas, s);
+}
+
+template status_t name_lms<uint8_t>(const uint8_t *, uint64_t, const uint32_t *, const uint32_t *, const uint32_t *,
+                                    uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t,
+                                    cudaStream_t);
+template status_t name_lms<uint32_t>(const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
+                                     const uint32_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *,
+                                     uint32_t *, uint32_t, cudaStream_t);
+
+__global__ void k_translate(uint32_t *red, uint64_t n1, const uint32_t *__restrict__ types,
+                            const uint32_t *__restrict__ heads, uint32_t *err) {
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n1; p += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = red[p];
+        if (c >= n1) {
+            dev_fail(err, DEVERR_RANGE);
+            red[p] = 0;
+            continue;
+        }
+        red[p] = bm_get(types, p) ? heads[c + 1] - 1 : heads[c];
+    }
+}
+
+status_t translate_names(uint32_t *red, uint64_t n1, const uint32_t *types, const uint32_t *heads, uint32_t *err,
+                         cudaStream_t s) {
+    if (n1 == 0) return PSACAK_OK;
+    uint64_t g = ceil_div(n1, 256);
+    k_translate<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(red, n1, types, heads, err);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
+// P[rank] = position for every LMS position.
+__global__ void k_lms_list(const uint32_t *__restrict__ lms, const uint32_t *__restrict__ pref, uint64_t nwords,
+                           uint32_t *plist) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t word = lms[w];
+        uint32_t o = pref[w];
+        while (word) {
+            int b = __ffs(word) - 1;
+            plist[o++] = (uint32_t)((w << 5) + b);
+            word &= word - 1;
+        }
+    }
+}
+
+__global__ void k_permute(uint32_t *sa1, uint64_t n1, const uint32_t *__restrict__ plist, uint32_t *err) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t r = sa1[i];
+        if (r >= n1) {
+            dev_fail(err, DEVERR_RANGE);
+            sa1[i] = 0;
+            continue;
+        }
+        sa1[i] = plist[r];
+    }
+}
+
+status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint32_t *lms_pref, uint64_t n,
+                     uint32_t *plist, uint32_t *err, cudaStream_t s) {
+    if (n1 == 0) return PSACAK_OK;
+    uint64_t nwords = ceil_div(n, 32);
+    uint64_t g = ceil_div(nwords, 256);
+    k_lms_list<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(lms, lms_pref, nwords, plist);
+    PSK_KCOUNT();
+    g = ceil_div(n1, 256);
+    k_permute<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(sa1, n1, plist, err);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
+__global__ void k_direct_inverse(const uint32_t *__restrict__ red, uint64_t n1, uint32_t *sa1, uint32_t *err) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = red[i];
+        if (c < n1) sa1[c] = (uint32_t)i;
+        else dev_fail(err, DEVERR_RANGE);
+    }
+}
+
+status_t direct_inverse(const uint32_t *red, uint64_t n1, uint32_t *sa1, uint32_t *err, cudaStream_t s) {
+    if (n1 == 0) return PSACAK_OK;
+    uint64_t g = ceil_div(n1, 256);
+    k_direct_inverse<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(red, n1, sa1, err);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
+// saca_tiny for n <= 3 (src/common.rs:13-25): insertion sort by suffix order.
+template <class C>
+__global__ void k_tiny_sa(const C *text, uint32_t n, uint32_t *sa) {
+    if (threadIdx.x || blockIdx.x) return;
+    uint32_t v[4];
+    for (uint32_t i = 0; i < n; i++) v[i] = i;
+    for (uint32_t i = 1; i < n; i++) {
+        for (uint32_t j = i; j > 0; j--) {
+            uint32_t a = v[j - 1], b = v[j];
+            // is suffix b < suffix a ?
+            uint32_t la = n - a, lb = n - b, k = 0;
+            bool less = false;
+            for (;; k++) {
+                if (k == lb) { less = (lb < la); break; }
+                if (k == la) { less = false; break; }
+                if (text[b + k] != text[a + k]) { less = text[b + k] < text[a + k]; break; }
+            }
+            if (!less) break;
+            v[j - 1] = b;
+            v[j] = a;
+        }
+    }
+    for (uint32_t i = 0; i < n; i++) sa[i] = v[i];
+}
+
+template <class C>
+status_t tiny_sa(const C *text, uint64_t n, uint32_t *sa, cudaStream_t s) {
+    if (n == 0) return PSACAK_OK;
+    if (n > 4) return set_error(PSACAK_EINTERNAL, "tiny_sa called with n=%llu", (unsigned long long)n);
+    k_tiny_sa<C><<<1, 32, 0, s>>>(text, (uint32_t)n, sa);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+template status_t tiny_sa<uint8_t>(const uint8_t *, uint64_t, uint32_t *, cudaStream_t);
+template status_t tiny_sa<uint32_t>(const uint32_t *, uint64_t, uint32_t *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Burkhardt-Kaerkkaeinen suffix-array check.
+// ---------------------------------------------------------------------------
+__global__ void k_check_isa(const uint32_t *__restrict__ sa, uint64_t n, uint32_t *isa, uint32_t *bad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t x = sa[i];
+        if (x >= n) {
+            atomicOr(bad, 1u);
+            continue;
+        }
+        uint32_t old = atomicExch(&isa[x], (uint32_t)i);
+        if (old != 0xFFFFFFFFu) atomicOr(bad, 2u);
+    }
+}
+
+template <class C>
+__global__ void k_check_order(const C *__restrict__ text, uint64_t n, const uint32_t *__restrict__ sa,
+                              const uint32_t *__restrict__ isa, uint32_t *bad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t a = sa[i - 1], b = sa[i];
+        if (a >= n || b >= n) continue;
+        C ca = text[a], cb = text[b];
+        if (ca > cb) {
+            atomicOr(bad, 4u);
+        } else if (ca == cb) {
+            int64_t ra = (a + 1 < n) ? (int64_t)isa[a + 1] : -1;
+            int64_t rb = (b + 1 < n) ? (int64_t)isa[b + 1] : -1;
+            if (ra >= rb) atomicOr(bad, 8u);
+        }
+    }
+}
+
+template <class C>
+status_t check_sa(const C *text, uint64_t n, const uint32_t *sa, uint32_t *isa, uint32_t *bad, cudaStream_t s) {
+    PSK_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
+    if (n == 0) return PSACAK_OK;
+    PSK_CUDA(cudaMemsetAsync(isa, 0xFF, n * sizeof(uint32_t), s));
+    uint64_t g = ceil_div(n, 256);
+    uint32_t grid = (uint32_t)(g < 16384 ? g : 16384);
+    k_check_isa<<<grid, 256, 0, s>>>(sa, n, isa, bad);
+    PSK_KCOUNT();
+    k_check_order<C><<<grid, 256, 0, s>>>(text, n, sa, isa, bad);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+template status_t check_sa<uint8_t>(const uint8_t *, uint64_t, const uint32_t *, uint32_t *, uint32_t *, cudaStream_t);
+template status_t check_sa<uint32_t>(const uint32_t *, uint64_t, const uint32_t *, uint32_t *, uint32_t *,
+                                     cudaStream_t);
+
+}  // namespace psk

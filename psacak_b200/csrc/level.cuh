@@ -1,0 +1,77 @@
+// level.cuh -- per-level kernels shared by every recursion level: L/S typing,
+// LMS bitmaps, naming of sorted LMS substrings, translation of names into
+// bucket pointers, permutation of the reduced suffix array, tiny levels.
+#pragma once
+
+#include "prims.cuh"
+
+namespace psk {
+
+// Positions per typing tile: 256 words of 32 positions.
+constexpr int TYPE_BLOCK = 256;
+constexpr uint64_t TYPE_TILE = 32ull * TYPE_BLOCK;
+
+struct Workspace;  // fwd
+
+// Histograms of a byte level: per character its count, its L-type count and
+// its LMS count (the reference's Buckets::new, src/psacak8.rs:355-374).
+struct ByteHist {
+    uint32_t count[256];
+    uint32_t lcount[256];
+    uint32_t lmscount[256];
+};
+
+// L/S typing of `text` into packed bitmaps: bit i of `types` is 1 iff
+// position i is S-type; bit i of `lms` is 1 iff position i is LMS.  Also
+// writes per-word LMS popcounts into `lms_wcnt` (nwords entries) and, for
+// bytes, accumulates `hist`.  `scratch` holds >= ntiles + 1024 uint32.
+template <class C>
+status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, uint32_t *lms_wcnt,
+                   ByteHist *hist, uint32_t *scratch, uint32_t max_ctas, cudaStream_t s);
+
+// Exclusive prefix of LMS popcounts: pref[w] = LMS positions before word w;
+// pref[nwords] = total, also copied to *total (device).
+status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *partial,
+                    uint32_t *total, uint32_t max_ctas, cudaStream_t s);
+
+// Rank of LMS position p among LMS positions (number of LMS before p).
+__device__ __forceinline__ uint32_t lms_rank(const uint32_t *lms, const uint32_t *pref, uint64_t p) {
+    uint32_t w = lms[p >> 5];
+    uint32_t below = (uint32_t)((1ull << (p & 31)) - 1);
+    return pref[p >> 5] + __popc(w & below);
+}
+
+// Names the n1 sorted LMS substrings `sorted` (positions in `text`) and
+// builds the reduced string: red[rank(p)] = name.  diff/name scratch of n1.
+// heads[c] = index in `sorted` where name c starts (k entries, then n1).
+// *k_out (device) = number of names.
+template <class C>
+status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t *lms_pref,
+                  const uint32_t *sorted, uint64_t n1, uint32_t *red, uint32_t *heads, uint32_t *flags,
+                  uint32_t *partial, uint32_t *k_out, uint32_t max_ctas, cudaStream_t s);
+
+// Translates names in `red` (types in `types`) into bucket pointers in place:
+// L -> heads[c], S -> heads[c+1] - 1 (the reference's translate,
+// src/naming.rs:263-274).  heads has k+1 entries (heads[k] = n1).
+status_t translate_names(uint32_t *red, uint64_t n1, const uint32_t *types, const uint32_t *heads,
+                         uint32_t *err, cudaStream_t s);
+
+// sa1[i] = P[sa1[i]] where P lists the LMS positions of `lms` in text order
+// (the reference's permutate_lmssuffixes, src/naming.rs:413-430).  `plist`
+// is scratch of n1 entries.
+status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint32_t *lms_pref, uint64_t n,
+                     uint32_t *plist, uint32_t *err, cudaStream_t s);
+
+// Direct inverse when all names are unique: sa1[red[i]] = i.
+status_t direct_inverse(const uint32_t *red, uint64_t n1, uint32_t *sa1, uint32_t *err, cudaStream_t s);
+
+// SA of a text of length <= 3 (saca_tiny for the reference's small cases).
+template <class C>
+status_t tiny_sa(const C *text, uint64_t n, uint32_t *sa, cudaStream_t s);
+
+// Burkhardt-Kaerkkaeinen check; *bad (device) receives 0 iff correct.
+template <class C>
+status_t check_sa(const C *text, uint64_t n, const uint32_t *sa, uint32_t *isa, uint32_t *bad,
+                  cudaStream_t s);
+
+}  // namespace psk

@@ -1,0 +1,108 @@
+"""GPU builds through the C ABI compared with the CPU oracle.
+
+Suffix arrays are integer permutations: every comparison here is exact.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as o
+import psacak_b200 as pk
+from psacak_b200 import synth
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+ENGINES = [pk.ENGINE_DOUBLING]
+
+
+def load(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = pk.Context(0)
+    yield c
+    c.close()
+
+
+def sched(engine):
+    return {"engine": engine, "inner_engine": pk.ENGINE_DOUBLING}
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_mississippi(ctx, engine):
+    assert ctx.psacak(b"mississippi", sched(engine)).tolist() == [10, 7, 4, 1, 0, 9, 8, 6, 3, 5, 2]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_reference_tables(ctx, engine):
+    for case in load("reference_vectors.json")["tables"]:
+        t = case["text"]
+        assert ctx.psacak(np.array(t, np.uint8), sched(engine)).tolist() == case["sa"], t
+        assert ctx.psacak32(np.array(t, np.uint32)).tolist() == case["sa"], t
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_edge_cases(ctx, engine):
+    cases = [b"", b"a", b"ab", b"ba", b"aaa", b"aaaa", b"abab", b"\xff\xff\xff\xff\xfe\xff",
+             bytes(range(255, -1, -1)), b"\x00" * 1000, b"ab" * 500, bytes([255]) * 77 + b"\x00",
+             b"\x00" * 70000, b"A" * 131073, bytes(range(256)) * 300]
+    for t in cases:
+        a = np.frombuffer(t, np.uint8)
+        assert (ctx.psacak(a, sched(engine)) == o.psacak8(a)).all(), t[:20]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_random_small_u8(ctx, engine):
+    rng = np.random.default_rng(20)
+    for _ in range(300):
+        n = int(rng.integers(0, 3000))
+        k = int(rng.choice([1, 2, 3, 4, 5, 16, 255, 256]))
+        t = rng.integers(0, k, n).astype(np.uint8)
+        got = ctx.psacak(t, sched(engine))
+        assert (got == o.psacak8(t)).all(), (n, k)
+
+
+def test_random_small_u32(ctx):
+    rng = np.random.default_rng(21)
+    for _ in range(300):
+        n = int(rng.integers(0, 3000))
+        k = int(rng.choice([1, 2, 7, 100, 5000, 1 << 20, 1 << 32]))
+        t = rng.integers(0, k, n, dtype=np.uint64).astype(np.uint32)
+        assert (ctx.psacak32(t) == o.psacak32(t)).all(), (n, k)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_synthetic_traces(ctx, engine):
+    from golden.make_golden import make_input
+    for case in load("synthetic_traces.json"):
+        t = make_input(case["generator"], case["n"], case["seed"])
+        if case["generator"] == "zipf32":
+            sa = ctx.psacak32(t)
+        else:
+            sa = ctx.psacak(t, sched(engine))
+        assert o.hash_u32(sa) == case["sa_hash"], case["name"]
+        assert ctx.trace() == case["levels"], case["name"]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_config1_8mib_acgt(ctx, engine):
+    t = synth.iid(8 << 20, b"ACGT", seed=1)
+    sa = ctx.psacak(t, sched(engine))
+    assert (sa == o.psacak8(t)).all()
+
+
+def test_genome_16mib(ctx):
+    t = synth.genome(16 << 20, seed=2)
+    sa = ctx.psacak(t)
+    assert (sa == o.psacak8(t)).all()
+
+
+def test_zipf32_4m(ctx):
+    t = synth.zipf32(4 << 20, seed=3)
+    sa = ctx.psacak32(t)
+    assert (sa == o.psacak32(t)).all()
