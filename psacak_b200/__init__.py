@@ -269,3 +269,47 @@ def psacak_inplace(text, suf):
 def psacak32(symbols):
     """Suffix array of an integer-alphabet string (uint32 symbols)."""
     return _ctx().psacak32(symbols)
+
+
+# -- internal stages (include/psacak_b200_debug.h) ---------------------------
+def _debug_lib():
+    L = lib()
+    if not getattr(L, "_debug_bound", False):
+        p, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+        L.psacak_debug_radix_sort_u64.argtypes = [p, p, p, u64, i32, i32]
+        L.psacak_debug_radix_sort_u32.argtypes = [p, p, p, u64, i32, i32]
+        L.psacak_debug_exclusive_sum.argtypes = [p, p, p, u64]
+        L.psacak_debug_types.argtypes = [p, p, u64, i32, p, p]
+        L.psacak_debug_reduced8.argtypes = [p, p, u64, p, u64, ctypes.POINTER(u64), ctypes.POINTER(u64), p]
+        for name in ("psacak_debug_radix_sort_u64", "psacak_debug_radix_sort_u32", "psacak_debug_exclusive_sum",
+                     "psacak_debug_types", "psacak_debug_reduced8"):
+            getattr(L, name).restype = i32
+        L._debug_bound = True
+    return L
+
+
+class Stages:
+    """Stage-level entry points on device pointers (ints), for tests/tuning."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.L = _debug_lib()
+
+    def radix_sort_u64(self, d_keys, d_vals, n, b0, b1):
+        _raise(self.L.psacak_debug_radix_sort_u64(self.ctx.handle, d_keys, d_vals, n, b0, b1))
+
+    def radix_sort_u32(self, d_keys, d_vals, n, b0, b1):
+        _raise(self.L.psacak_debug_radix_sort_u32(self.ctx.handle, d_keys, d_vals, n, b0, b1))
+
+    def exclusive_sum(self, d_in, d_out, n):
+        _raise(self.L.psacak_debug_exclusive_sum(self.ctx.handle, d_in, d_out, n))
+
+    def types(self, d_text, n, width, d_types, d_lms):
+        _raise(self.L.psacak_debug_types(self.ctx.handle, d_text, n, width, d_types, d_lms))
+
+    def reduced8(self, d_text, n, d_red, cap, schedule=None):
+        n1 = ctypes.c_uint64(0)
+        k = ctypes.c_uint64(0)
+        _raise(self.L.psacak_debug_reduced8(self.ctx.handle, d_text, n, d_red, cap, ctypes.byref(n1),
+                                            ctypes.byref(k), _sched_ptr(schedule)))
+        return int(n1.value), int(k.value)

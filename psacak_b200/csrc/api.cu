@@ -7,6 +7,7 @@
 
 #include "ctx.cuh"
 #include "induce.cuh"
+#include "../../include/psacak_b200_debug.h"
 
 namespace psk {
 
@@ -225,18 +226,38 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
                 PSK_TRY(translate_names(red, n1, t1, heads, ctx.d_err, s));
             }
             heads.reset();
+            if (level == 0 && ctx.debug_red) {
+                uint64_t c = n1 < ctx.debug_cap ? n1 : ctx.debug_cap;
+                PSK_CUDA(cudaMemcpyAsync(ctx.debug_red, red.get(), c * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+                ctx.debug_n1 = n1;
+                ctx.debug_k = k;
+                return ctx.sync();
+            }
             uint64_t hsh = 0;
             PSK_TRY(hash_device(ctx, red, n1, &hsh));
             trace_push(ctx, level, width, n, n1, k, hsh);
             PSK_TRY(build_level<uint32_t>(ctx, red, n1, sa1, level + 1));
         } else {
             heads.reset();
+            if (level == 0 && ctx.debug_red) {
+                // all names unique: the reduced string is the name string
+                uint64_t c = n1 < ctx.debug_cap ? n1 : ctx.debug_cap;
+                PSK_CUDA(cudaMemcpyAsync(ctx.debug_red, red.get(), c * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+                ctx.debug_n1 = n1;
+                ctx.debug_k = k;
+                return ctx.sync();
+            }
             trace_push(ctx, level, width, n, n1, k, 0);
             PSK_TRY(direct_inverse(red, n1, sa1, ctx.d_err, s));
         }
         // red is free again; reuse it as the position list of the permutation.
         PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
     } else {
+        if (level == 0 && ctx.debug_red) {
+            ctx.debug_n1 = 0;
+            ctx.debug_k = 0;
+            return ctx.sync();
+        }
         trace_push(ctx, level, width, n, 0, 0, 0);
     }
     red.reset();
@@ -615,6 +636,120 @@ int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *
         if (rc) return rc;
     }
     return PSACAK_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Debug / stage entry points (include/psacak_b200_debug.h).
+// ---------------------------------------------------------------------------
+__global__ void k_copy_u64(const uint64_t *a, uint64_t *b, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+struct CopyLoad {
+    const uint32_t *in;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return in[i]; }
+};
+struct CopyStore {
+    uint32_t *out;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t) const { out[i] = excl; }
+};
+
+template <class K>
+static int debug_sort(psacak_ctx *ctx, K *keys, uint32_t *vals, uint64_t n, int b0, int b1) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = c.own_stream;
+    DBuf<K> k1;
+    DBuf<uint32_t> v1;
+    PSK_TRY(k1.init(c, n));
+    PSK_TRY(v1.init(c, n));
+    int in1 = 0;
+    PSK_TRY((radix_sort_pairs<K, uint32_t>(keys, vals, k1, v1, n, b0, b1, c.d_hist, &in1, c.radix_ctas, c.stream)));
+    if (in1) {
+        PSK_CUDA(cudaMemcpyAsync(keys, k1.get(), n * sizeof(K), cudaMemcpyDeviceToDevice, c.stream));
+        PSK_CUDA(cudaMemcpyAsync(vals, v1.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));
+    }
+    k1.reset();
+    v1.reset();
+    PSK_TRY(c.sync());
+    return c.check_device_error();
+}
+
+extern "C" {
+
+int psacak_debug_radix_sort_u64(psacak_ctx *ctx, uint64_t *d_keys, uint32_t *d_vals, uint64_t n, int begin_bit,
+                                int end_bit) {
+    return debug_sort<uint64_t>(ctx, d_keys, d_vals, n, begin_bit, end_bit);
+}
+
+int psacak_debug_radix_sort_u32(psacak_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals, uint64_t n, int begin_bit,
+                                int end_bit) {
+    return debug_sort<uint32_t>(ctx, d_keys, d_vals, n, begin_bit, end_bit);
+}
+
+int psacak_debug_exclusive_sum(psacak_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint64_t n) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = c.own_stream;
+    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(CopyLoad{d_in}, CopyStore{d_out}, n, c.d_partial,
+                                                   (uint32_t *)nullptr, OpSum<uint32_t>(), c.scan_ctas, c.stream)));
+    return c.sync();
+}
+
+int psacak_debug_types(psacak_ctx *ctx, const void *d_text, uint64_t n, int width, uint32_t *d_types,
+                       uint32_t *d_lms) {
+    clear_error();
+    if (!ctx || (width != 1 && width != 4)) return set_error(PSACAK_EINVAL, "bad context or width");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = c.own_stream;
+    DBuf<uint32_t> wcnt, scr;
+    DBuf<ByteHist> hist;
+    PSK_TRY(wcnt.init(c, ceil_div(n, 32) + 1));
+    PSK_TRY(scr.init(c, 2 * ceil_div(n, TYPE_TILE) + 1024));
+    PSK_TRY(hist.init(c, 1));
+    if (width == 1)
+        PSK_TRY(type_text<uint8_t>((const uint8_t *)d_text, n, d_types, d_lms, wcnt, hist, scr, c.scan_ctas, c.stream));
+    else
+        PSK_TRY(type_text<uint32_t>((const uint32_t *)d_text, n, d_types, d_lms, wcnt, nullptr, scr, c.scan_ctas,
+                                    c.stream));
+    return c.sync();
+}
+
+int psacak_debug_reduced8(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, uint32_t *d_red, uint64_t cap,
+                          uint64_t *n_lms, uint64_t *k, const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx || !n_lms || !k) return set_error(PSACAK_EINVAL, "null argument");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = c.own_stream;
+    apply_schedule(c, sched);
+    c.trace.clear();
+    c.debug_red = d_red;
+    c.debug_cap = cap;
+    c.debug_n1 = c.debug_k = 0;
+    status_t st = PSACAK_OK;
+    if (n > 3) {
+        DBuf<uint32_t> sa;
+        st = sa.init(c, n);
+        if (st == PSACAK_OK) st = build_level<uint8_t>(c, d_text, n, sa, 0);
+    }
+    c.debug_red = nullptr;
+    if (st != PSACAK_OK) return st;
+    *n_lms = c.debug_n1;
+    *k = c.debug_k;
+    PSK_TRY(c.sync());
+    return c.check_device_error();
 }
 
 }  // extern "C"

@@ -24,6 +24,10 @@ struct Ctx {
     uint32_t scan_ctas = 0;         // CTAs of the chunked scans
     uint32_t radix_ctas = 0;        // CTAs of the radix passes
     psacak_schedule sched{};
+    // When set, level 0 stops after building its reduced string and copies
+    // it here (used by psacak_debug_reduced8).
+    uint32_t *debug_red = nullptr;
+    uint64_t debug_cap = 0, debug_n1 = 0, debug_k = 0;
     std::vector<psacak_level_info> trace;
     std::mutex mu;
 

@@ -93,15 +93,25 @@ __global__ void __launch_bounds__(TYPE_BLOCK) k_type_main(const C *__restrict__ 
             }
             if (HIST) pk[it >> 2] |= ((uint32_t)(uint8_t)a) << ((it & 3) * 8);
         }
-        // nearest change point to the right of this word within the tile
-        const uint32_t r = TYPE_BLOCK - 1 - threadIdx.x;
+        // Nearest change point to the right of this word within the tile: an
+        // exclusive max-scan run in reversed word order (scan slot u holds
+        // word 255-u), each value tagged with its slot so the max picks the
+        // nearest word.
+        const uint32_t u = TYPE_BLOCK - 1 - threadIdx.x;
         uint32_t enc = 0;
         if (myC) {
             int lb = __ffs(myC) - 1;
-            enc = ((r + 1) << 1) | ((myD >> lb) & 1u);
+            enc = ((u + 1) << 1) | ((myD >> lb) & 1u);
         }
-        uint32_t excl;
-        block_scan<uint32_t, OpMax<uint32_t>, TYPE_BLOCK>(enc, OpMax<uint32_t>(), s_scan, &excl, (uint32_t *)nullptr);
+        s_hi[u] = enc;
+        __syncthreads();
+        uint32_t rv = s_hi[threadIdx.x];
+        uint32_t rex;
+        block_scan<uint32_t, OpMax<uint32_t>, TYPE_BLOCK>(rv, OpMax<uint32_t>(), s_scan, &rex, (uint32_t *)nullptr);
+        s_hi[TYPE_BLOCK - 1 - threadIdx.x] = rex;
+        __syncthreads();
+        uint32_t excl = s_hi[threadIdx.x];
+        __syncthreads();
         uint32_t cur = excl ? (excl & 1u) : tile_carry[tile];
         uint32_t T = 0;
 #pragma unroll
