@@ -98,7 +98,7 @@ static void trace_push(Ctx &ctx, uint32_t level, uint32_t width, uint64_t m, uin
 static int engine_for(const Ctx &ctx, uint32_t level, bool bytes) {
     uint32_t e = level == 0 ? ctx.sched.engine : ctx.sched.inner_engine;
     if (e == PSACAK_ENGINE_BUCKET && !bytes) e = PSACAK_ENGINE_DOUBLING;
-    if (e == PSACAK_ENGINE_AUTO) e = PSACAK_ENGINE_DOUBLING;
+    if (e == PSACAK_ENGINE_AUTO) e = bytes ? PSACAK_ENGINE_BUCKET : PSACAK_ENGINE_DOUBLING;
     return (int)e;
 }
 
@@ -181,7 +181,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
     // Stage 1: sort the LMS substrings.
     if constexpr (sizeof(C) == 1) {
         if (engine == PSACAK_ENGINE_BUCKET)
-            PSK_TRY(induce_bucket8(ctx, text, n, types, hg, dgeom.get(), INDUCE_LMS_SUBSTRINGS, nullptr, n1, sa, s));
+            PSK_TRY(induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_LMS_SUBSTRINGS, nullptr, n1, sa, s));
         else
             PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_LMS_SUBSTRINGS, nullptr, n1, cursor,
                                        sa, s));
@@ -265,7 +265,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
     // Stage 3: induce the whole suffix array from the sorted LMS suffixes.
     if constexpr (sizeof(C) == 1) {
         if (engine == PSACAK_ENGINE_BUCKET)
-            return induce_bucket8(ctx, text, n, types, hg, dgeom.get(), INDUCE_FINAL, sa1, n1, sa, s);
+            return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sa1, n1, sa, s);
         return induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
     } else {
         return induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_FINAL, sa1, n1, nullptr, sa, s);

@@ -14,7 +14,7 @@ from psacak_b200 import synth
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-ENGINES = [pk.ENGINE_DOUBLING]
+ENGINES = [pk.ENGINE_BUCKET, pk.ENGINE_DOUBLING]
 
 
 def load(name):

@@ -118,10 +118,16 @@ def test_types_u32(st, n, k):
     _types_case(st, rng.integers(0, k, n).astype(np.uint32), 4)
 
 
-@pytest.mark.parametrize("gen,n", [("iid3", 2676), ("iid4", 100_000), ("genome", 1 << 20), ("iid256", 300_000)])
-def test_reduced_string_level0(st, gen, n):
+@pytest.mark.parametrize("engine", [pk.ENGINE_BUCKET, pk.ENGINE_DOUBLING])
+@pytest.mark.parametrize("gen,n", [("iid3", 2676), ("iid4", 100_000), ("genome", 1 << 20), ("iid256", 300_000),
+                                   ("runs", 200_000)])
+def test_reduced_string_level0(st, gen, n, engine):
     if gen == "genome":
         t = synth.genome(n, seed=9)
+    elif gen == "runs":
+        rng = np.random.default_rng(3)
+        t = np.repeat(rng.integers(0, 3, n // 50).astype(np.uint8), rng.integers(1, 100, n // 50))[:n]
+        n = t.size
     else:
         k = int(gen[3:])
         t = np.random.default_rng(n).integers(0, k, n).astype(np.uint8)
@@ -129,6 +135,6 @@ def test_reduced_string_level0(st, gen, n):
     dt = dev(t)
     dr = torch.zeros(max(want.size, 1), dtype=torch.int32, device="cuda")
     n1, k = st.reduced8(dt.data_ptr(), n, dr.data_ptr(), want.size,
-                        {"engine": pk.ENGINE_DOUBLING, "inner_engine": pk.ENGINE_DOUBLING})
+                        {"engine": engine, "inner_engine": pk.ENGINE_DOUBLING})
     assert (n1, k) == (want.size, wk)
     assert (dr.cpu().numpy().view(np.uint32)[:n1] == want).all()
