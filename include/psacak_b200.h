@@ -129,6 +129,23 @@ PSACAK_API int psacak_check_sa8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint
 PSACAK_API int psacak_check_sa32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n,
                           const uint32_t *d_sa, int *ok, void *stream);
 
+/* Per-kernel-class device time of the builds made while profiling is on
+ * (CUDA events around every launch; adds a little host overhead).
+ * `bytes` is the algorithmic traffic of the class: the bytes its launches
+ * must move by construction (each input read once, each output written
+ * once), independent of caching. */
+typedef struct {
+    char name[32];
+    uint64_t launches;
+    uint64_t items;   /* units processed (entries, positions, keys) */
+    uint64_t bytes;   /* algorithmic bytes, 0 where not defined */
+    double ms;        /* summed device time */
+} psacak_kernel_stat;
+
+PSACAK_API int psacak_profile_enable(psacak_ctx *ctx, int on);
+PSACAK_API int psacak_profile_reset(psacak_ctx *ctx);
+PSACAK_API int psacak_profile_get(psacak_ctx *ctx, psacak_kernel_stat *out, uint32_t cap, uint32_t *count);
+
 /* Number of kernels the library launched since the context was created. */
 PSACAK_API uint64_t psacak_kernel_launches(psacak_ctx *ctx);
 

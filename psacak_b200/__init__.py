@@ -63,6 +63,16 @@ class Schedule(ctypes.Structure):
     ]
 
 
+class KernelStat(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("launches", ctypes.c_uint64),
+        ("items", ctypes.c_uint64),
+        ("bytes", ctypes.c_uint64),
+        ("ms", ctypes.c_double),
+    ]
+
+
 class LevelInfo(ctypes.Structure):
     _fields_ = [
         ("level", ctypes.c_uint32),
@@ -107,11 +117,15 @@ def lib():
         L.psacak_get_trace.argtypes = [p, p, u32, ctypes.POINTER(u32)]
         L.psacak_check_sa8_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
         L.psacak_check_sa32_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
+        L.psacak_profile_enable.argtypes = [p, i32]
+        L.psacak_profile_reset.argtypes = [p]
+        L.psacak_profile_get.argtypes = [p, p, u32, ctypes.POINTER(u32)]
         L.psacak_kernel_launches.argtypes = [p]
         L.psacak_kernel_launches.restype = u64
         for name in ("psacak8", "psacak32", "psacak8_ctx", "psacak32_ctx", "psacak8_dev", "psacak32_dev",
                      "psacak8_batch", "psacak_get_trace", "psacak_check_sa8_dev", "psacak_check_sa32_dev",
-                     "psacak_ctx_create", "psacak_ctx_destroy"):
+                     "psacak_ctx_create", "psacak_ctx_destroy", "psacak_profile_enable", "psacak_profile_reset",
+                     "psacak_profile_get"):
             getattr(L, name).restype = i32
         _lib = L
         return L
@@ -224,6 +238,19 @@ class Context:
 
     def kernel_launches(self):
         return int(lib().psacak_kernel_launches(self._h))
+
+    def profile(self, on=True):
+        _raise(lib().psacak_profile_enable(self._h, 1 if on else 0))
+
+    def profile_reset(self):
+        _raise(lib().psacak_profile_reset(self._h))
+
+    def profile_stats(self):
+        buf = (KernelStat * 128)()
+        cnt = ctypes.c_uint32(0)
+        _raise(lib().psacak_profile_get(self._h, buf, 128, ctypes.byref(cnt)))
+        return [dict(name=s.name.decode(), launches=s.launches, items=s.items, bytes=s.bytes, ms=s.ms)
+                for s in buf[:min(cnt.value, 128)]]
 
 
 def _sched_ptr(schedule):

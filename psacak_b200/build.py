@@ -84,7 +84,7 @@ def build_synth():
     src = os.path.join(CSRC, "synth.c")
     out = os.path.join(LIB, "libpsacak_synth.so")
     if _stale(out, [src]):
-        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-o", out, src, "-lm"])
+        subprocess.check_call(["gcc", "-O3", "-march=x86-64-v2", "-fPIC", "-shared", "-o", out, src, "-lm"])
     return out
 
 

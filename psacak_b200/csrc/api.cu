@@ -400,6 +400,8 @@ status_t ctx_init(Ctx &c, int device) {
     PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_err, sizeof(uint32_t)));
     PSK_CUDA(cudaMemset(c.d_err, 0, sizeof(uint32_t)));
+    PSK_CUDA(cudaMalloc(&c.d_induced, sizeof(unsigned long long)));
+    PSK_CUDA(cudaMemset(c.d_induced, 0, sizeof(unsigned long long)));
     c.scan_ctas = 4 * (uint32_t)c.dev.num_sms;
     c.radix_ctas = 4 * (uint32_t)c.dev.num_sms;
     if (c.scan_ctas > MAX_CHUNKS) c.scan_ctas = MAX_CHUNKS;
@@ -413,6 +415,7 @@ void ctx_free(Ctx &c) {
     if (c.d_hist) cudaFree(c.d_hist);
     if (c.d_scalars) cudaFree(c.d_scalars);
     if (c.d_err) cudaFree(c.d_err);
+    if (c.d_induced) cudaFree(c.d_induced);
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
     c.h_pinned = nullptr;
 }
@@ -427,6 +430,29 @@ static void apply_schedule(Ctx &c, const psacak_schedule *sched) {
 }
 
 // Common body of the device-pointer entry points.
+// Sets the thread's profiler hook for the duration of one public call.
+struct ProfGuard {
+    Ctx &c;
+    explicit ProfGuard(Ctx &cc) : c(cc) { t_prof = c.profiling ? &c.prof : nullptr; }
+    ~ProfGuard() { t_prof = nullptr; }
+};
+
+// Folds the device-side count of entries scattered by the bucket scans into
+// the "induce_down" class (4 bytes read + 4 bytes written per entry).
+static status_t profile_collect(Ctx &c) {
+    if (!c.profiling) return PSACAK_OK;
+    c.prof.resolve();
+    uint32_t h[2];
+    PSK_TRY(c.read_u32((const uint32_t *)c.d_induced, h, 2));
+    PSK_CUDA(cudaMemsetAsync(c.d_induced, 0, sizeof(unsigned long long), c.stream));
+    unsigned long long induced = ((unsigned long long)h[1] << 32) | h[0];
+    if (induced) {
+        int cls = c.prof.cls_of("induce_down");
+        c.prof.stats[cls].bytes += 8ull * induced;
+    }
+    return PSACAK_OK;
+}
+
 template <class C>
 status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream_t stream,
                  const psacak_schedule *sched) {
@@ -434,6 +460,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     c.stream = stream ? stream : c.own_stream;
     apply_schedule(c, sched);
     c.trace.clear();
+    ProfGuard pg(c);
     status_t st;
     if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, n, d_sa, 0);
     else st = build_psacak32(c, d_text, n, d_sa);
@@ -443,6 +470,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     }
     PSK_TRY(c.sync());
     PSK_TRY(c.check_device_error());
+    PSK_TRY(profile_collect(c));
     return PSACAK_OK;
 }
 
@@ -619,6 +647,37 @@ int psacak_check_sa8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, con
 int psacak_check_sa32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, const uint32_t *d_sa, int *ok,
                           void *stream) {
     return check_dev<uint32_t>(ctx, d_text, n, d_sa, ok, stream);
+}
+
+int psacak_profile_enable(psacak_ctx *ctx, int on) {
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    ctx->c.profiling = on != 0;
+    return PSACAK_OK;
+}
+
+int psacak_profile_reset(psacak_ctx *ctx) {
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    ctx->c.prof.reset();
+    return PSACAK_OK;
+}
+
+int psacak_profile_get(psacak_ctx *ctx, psacak_kernel_stat *out, uint32_t cap, uint32_t *count) {
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    const auto &st = ctx->c.prof.stats;
+    uint32_t n = (uint32_t)st.size();
+    for (uint32_t i = 0; i < n && i < cap && out; i++) {
+        memset(&out[i], 0, sizeof(out[i]));
+        strncpy(out[i].name, st[i].name, sizeof(out[i].name) - 1);
+        out[i].launches = st[i].launches;
+        out[i].items = st[i].items;
+        out[i].bytes = st[i].bytes;
+        out[i].ms = st[i].ms;
+    }
+    if (count) *count = n;
+    return PSACAK_OK;
 }
 
 uint64_t psacak_kernel_launches(psacak_ctx *ctx) {

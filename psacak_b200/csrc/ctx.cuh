@@ -29,6 +29,9 @@ struct Ctx {
     uint32_t *debug_red = nullptr;
     uint64_t debug_cap = 0, debug_n1 = 0, debug_k = 0;
     std::vector<psacak_level_info> trace;
+    bool profiling = false;
+    Profiler prof;
+    unsigned long long *d_induced = nullptr;  // entries scattered by the bucket scans
     std::mutex mu;
 
     template <class T>

@@ -178,15 +178,17 @@ __global__ void __launch_bounds__(MS_BLOCK) k_ms_up(const uint8_t *__restrict__ 
 }
 
 // Turns the histograms into per-CTA start slots and advances the cursors.
-__global__ void k_ms_offsets(uint32_t *hist, uint32_t G, uint32_t *cursor, int dir) {
+__global__ void k_ms_offsets(uint32_t *hist, uint32_t G, uint32_t *cursor, int dir, unsigned long long *induced) {
     int d = threadIdx.x;
-    uint32_t run = cursor[d];
+    uint32_t run = cursor[d], tot = 0;
     for (uint32_t b = 0; b < G; b++) {
         uint32_t h = hist[(uint64_t)d * G + b];
         hist[(uint64_t)d * G + b] = run;
         run = dir > 0 ? run + h : run - h;
+        tot += h;
     }
     cursor[d] = run;
+    if (tot) atomicAdd(induced, (unsigned long long)tot);
 }
 
 template <bool LSCAN>
@@ -292,8 +294,8 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     uint32_t *d_max = ctx.d_scalars + 8;
     uint32_t *d_tot = ctx.d_scalars + 9;
     PSK_CUDA(cudaMemsetAsync(d_max, 0, sizeof(uint32_t), s));
-    k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_max);
-    PSK_KCOUNT();
+    PSK_PROF_LAUNCH(s, "chain_runs", nseeds, 0,
+                    (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_max)));
     PSK_LAUNCH_CHECK();
     PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(RunLoad{runs}, RunStore{off}, nseeds, ctx.d_partial, d_tot,
                                                    OpSum<uint32_t>(), ctx.scan_ctas, s)));
@@ -302,15 +304,15 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     const uint32_t maxrun = h[0], ncells = h[1];
     if (nseeds + ncells != part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds + %u chained != %u", c, nseeds, ncells, part);
-    k_expand_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, ncells, k0, v0);
-    PSK_KCOUNT();
+    PSK_PROF_LAUNCH(s, "chain_expand", ncells, 0,
+                    (k_expand_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, ncells, k0, v0)));
     PSK_LAUNCH_CHECK();
     int in1 = 0;
     PSK_TRY((radix_sort_pairs<uint32_t, uint32_t>(k0, v0, k1, v1, ncells, 0, bitlen(maxrun), ctx.d_hist, &in1,
                                                   ctx.radix_ctas, s)));
     uint32_t first = dir > 0 ? start + nseeds : start - nseeds;
-    k_place_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(in1 ? v1 : v0, ncells, first, dir, sa);
-    PSK_KCOUNT();
+    PSK_PROF_LAUNCH(s, "chain_place", ncells, 8ull * ncells,
+                    (k_place_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(in1 ? v1 : v0, ncells, first, dir, sa)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -321,12 +323,18 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
     uint32_t nitems = seq.a_len + seq.b_len;
     if (nitems == 0) return PSACAK_OK;
     Chunking ch = make_chunking(nitems, MS_TILE, ctx.radix_ctas < RADIX_MAX_CTAS ? ctx.radix_ctas : RADIX_MAX_CTAS);
-    k_ms_up<LSCAN><<<ch.G, MS_BLOCK, 0, s>>>(text, sa, seq, nitems, c, ch.chunk, dg, ctx.d_hist, ch.G);
-    PSK_KCOUNT();
-    k_ms_offsets<<<1, 256, 0, s>>>(ctx.d_hist, ch.G, cursor, LSCAN ? 1 : -1);
-    PSK_KCOUNT();
-    k_ms_down<LSCAN><<<ch.G, MS_BLOCK, 0, s>>>(sa, seq, nitems, ch.chunk, dg, ctx.d_hist, ch.G, sa, n, ctx.d_err);
-    PSK_KCOUNT();
+    // algorithmic bytes: up reads each entry (4) and its predecessor's
+    // character (1) and writes the digit (1); down reads the digit (1) and,
+    // for inducing entries, the entry (4) and writes it to its bucket (4) --
+    // the inducing count is added from the device at the end of the build.
+    PSK_PROF_LAUNCH(s, "induce_up", nitems, 6ull * nitems,
+                    (k_ms_up<LSCAN><<<ch.G, MS_BLOCK, 0, s>>>(text, sa, seq, nitems, c, ch.chunk, dg, ctx.d_hist,
+                                                              ch.G)));
+    PSK_PROF_LAUNCH(s, "induce_offsets", 256, 0,
+                    (k_ms_offsets<<<1, 256, 0, s>>>(ctx.d_hist, ch.G, cursor, LSCAN ? 1 : -1, ctx.d_induced)));
+    PSK_PROF_LAUNCH(s, "induce_down", nitems, 1ull * nitems,
+                    (k_ms_down<LSCAN><<<ch.G, MS_BLOCK, 0, s>>>(sa, seq, nitems, ch.chunk, dg, ctx.d_hist, ch.G, sa, n,
+                                                                ctx.d_err)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -357,11 +365,11 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
     if (mode == INDUCE_LMS_SUBSTRINGS) {
         PSK_CUDA(cudaMemsetAsync(curL, 0, 256 * sizeof(uint32_t), s));
         const uint64_t nwords = ceil_div(n, 32);
-        k_place_lms_any8<<<grid_cap(nwords, 8192), 256, 0, s>>>(text, nwords, lms, dgeom, curL, sa);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "place_lms", nwords, 0,
+                        (k_place_lms_any8<<<grid_cap(nwords, 8192), 256, 0, s>>>(text, nwords, lms, dgeom, curL, sa)));
     } else if (n1 > 0) {
-        k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(text, sorted_lms, n1, dgeom, sa);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "place_lms", n1, 0,
+                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(text, sorted_lms, n1, dgeom, sa)));
     }
     k_init_cursors<<<1, 256, 0, s>>>(dgeom, text, n, curL, curS, sa);
     PSK_KCOUNT();

@@ -193,9 +193,9 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
     for (uint64_t h = 1; cnt > 0; h <<= 1) {
         if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
         uint64_t gblocks = ceil_div(cnt, 256);
-        k_keys<<<(uint32_t)(gblocks < 16384 ? gblocks : 16384), 256, 0, s>>>(Wg, Wv, cnt, R, n, h, KB, k0, v0,
-                                                                             ctx.d_err);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
+                        (k_keys<<<(uint32_t)(gblocks < 16384 ? gblocks : 16384), 256, 0, s>>>(Wg, Wv, cnt, R, n, h, KB,
+                                                                                              k0, v0, ctx.d_err)));
         PSK_LAUNCH_CHECK();
         int in1 = 0;
         PSK_TRY((radix_sort_pairs<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, ctx.d_hist, &in1,
@@ -228,8 +228,9 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
     const uint64_t nwords = ceil_div(n, 32);
     if (mode == INDUCE_LMS_SUBSTRINGS) {
         uint64_t g = ceil_div(nwords, 256);
-        k_place_lms_any<C><<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(text, nwords, lms, geom, cursor, R);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "place_lms", nwords, 0,
+                        (k_place_lms_any<C><<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(text, nwords, lms, geom,
+                                                                                            cursor, R)));
         PSK_LAUNCH_CHECK();
     } else if (n1 > 0) {
         PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{text, sorted_lms, n1, geom},

@@ -182,18 +182,22 @@ status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, ui
     uint32_t *carry = scratch + ntiles;
     uint32_t *partial = scratch + 2 * ntiles;
     uint32_t grid = (uint32_t)(ntiles < max_ctas ? ntiles : max_ctas);
-    k_tile_first<C><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, code);
-    PSK_KCOUNT();
+    PSK_PROF_LAUNCH(s, "type_tile_first", ntiles, 0, (k_tile_first<C><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, code)));
     PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(TileCarryLoad{code, ntiles}, TileCarryStore{carry, ntiles},
                                                    ntiles, partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
                                                    max_ctas, s)));
+    // algorithmic bytes: the text once, two bitmaps and the word counts
+    const uint64_t tbytes = n * sizeof(C) + 3 * ceil_div(n, 32) * 4;
     if (hist) {
         PSK_CUDA(cudaMemsetAsync(hist, 0, sizeof(ByteHist), s));
-        k_type_main<C, true><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, carry, types, lms, lms_wcnt, hist);
+        PSK_PROF_LAUNCH(s, "type_main", n, tbytes,
+                        (k_type_main<C, true><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, carry, types, lms, lms_wcnt,
+                                                                         hist)));
     } else {
-        k_type_main<C, false><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, carry, types, lms, lms_wcnt, nullptr);
+        PSK_PROF_LAUNCH(s, "type_main", n, tbytes,
+                        (k_type_main<C, false><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, carry, types, lms,
+                                                                          lms_wcnt, nullptr)));
     }
-    PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -293,8 +297,7 @@ status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t
         return PSACAK_OK;
     }
     uint32_t grid = (uint32_t)(ceil_div(n1, 256) < (uint64_t)max_ctas * 4 ? ceil_div(n1, 256) : (uint64_t)max_ctas * 4);
-    k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lms, sorted, n1, flags);
-    PSK_KCOUNT();
+    PSK_PROF_LAUNCH(s, "name_flags", n1, 0, (k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lms, sorted, n1, flags)));
     PSK_LAUNCH_CHECK();
     return chunk_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags}, NameStore{sorted, lms, lms_pref, red, heads, n1},
                                                  n1, partial, k_out, OpSum<uint32_t>(), max_ctas, s);

@@ -9,6 +9,7 @@
 namespace psk {
 
 std::atomic<uint64_t> g_kernel_launches{0};
+thread_local Profiler *t_prof = nullptr;
 
 static thread_local char t_last_error[512] = "";
 

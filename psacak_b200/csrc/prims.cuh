@@ -13,6 +13,9 @@ namespace psk {
 
 extern std::atomic<uint64_t> g_kernel_launches;
 #define PSK_KCOUNT() (::psk::g_kernel_launches.fetch_add(1, std::memory_order_relaxed))
+}  // namespace psk
+#include "prof.cuh"
+namespace psk {
 
 constexpr int SCAN_BLOCK = 256;
 constexpr int SCAN_IPT = 8;
@@ -152,14 +155,14 @@ status_t chunk_scan(Load ld, Store st, uint64_t n, T *partial, T *total_out, Op 
                     uint32_t max_ctas, cudaStream_t s) {
     Chunking c = make_chunking(n, SCAN_TILE, max_ctas < MAX_CHUNKS ? max_ctas : MAX_CHUNKS);
     if (n > 0) {
-        k_chunk_reduce<T, Op, Load><<<c.G, SCAN_BLOCK, 0, s>>>(ld, n, c.chunk, partial, op);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "scan_reduce", n, 0,
+                        (k_chunk_reduce<T, Op, Load><<<c.G, SCAN_BLOCK, 0, s>>>(ld, n, c.chunk, partial, op)));
     }
-    k_scan_partials<T, Op><<<1, 1024, 0, s>>>(partial, n > 0 ? c.G : 0, total_out, op);
-    PSK_KCOUNT();
+    PSK_PROF_LAUNCH(s, "scan_partials", c.G, 0,
+                    (k_scan_partials<T, Op><<<1, 1024, 0, s>>>(partial, n > 0 ? c.G : 0, total_out, op)));
     if (n > 0) {
-        k_chunk_scan<T, Op, Load, Store><<<c.G, SCAN_BLOCK, 0, s>>>(ld, st, n, c.chunk, partial, op);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "scan_apply", n, 0,
+                        (k_chunk_scan<T, Op, Load, Store><<<c.G, SCAN_BLOCK, 0, s>>>(ld, st, n, c.chunk, partial, op)));
     }
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
@@ -328,12 +331,12 @@ status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit,
     for (int shift = begin_bit; shift < end_bit; shift += 8) {
         int bits = end_bit - shift < 8 ? end_bit - shift : 8;
         uint32_t dmask = (1u << bits) - 1;
-        k_radix_upsweep<K><<<c.G, RADIX_BLOCK, 0, s>>>(ki, n, c.chunk, shift, dmask, hist, c.G);
-        PSK_KCOUNT();
-        k_radix_scan<<<1, 1024, 0, s>>>(hist, 256 * c.G);
-        PSK_KCOUNT();
-        k_radix_downsweep<K, V><<<c.G, RADIX_BLOCK, smem, s>>>(ki, vi, ko, vo, n, c.chunk, shift, dmask, hist, c.G);
-        PSK_KCOUNT();
+        PSK_PROF_LAUNCH(s, "radix_upsweep", n, n * sizeof(K),
+                        (k_radix_upsweep<K><<<c.G, RADIX_BLOCK, 0, s>>>(ki, n, c.chunk, shift, dmask, hist, c.G)));
+        PSK_PROF_LAUNCH(s, "radix_scan", 256 * c.G, 0, (k_radix_scan<<<1, 1024, 0, s>>>(hist, 256 * c.G)));
+        PSK_PROF_LAUNCH(s, "radix_downsweep", n, 2 * n * (sizeof(K) + sizeof(V)),
+                        (k_radix_downsweep<K, V><<<c.G, RADIX_BLOCK, smem, s>>>(ki, vi, ko, vo, n, c.chunk, shift,
+                                                                                 dmask, hist, c.G)));
         PSK_LAUNCH_CHECK();
         K *tk = ki; ki = ko; ko = tk;
         V *tv = vi; vi = vo; vo = tv;

@@ -121,6 +121,20 @@ static inline uint8_t markov_draw(xo_t *r, const double *row) {
     return ACGT[b];
 }
 
+/* Integer form of a Markov table: per context three 32-bit thresholds. */
+static void markov_thresholds(const double *cum, uint32_t *thr, int ctx) {
+    for (int c = 0; c < ctx; c++)
+        for (int b = 0; b < 3; b++) {
+            double v = cum[c * 4 + b] * 4294967296.0;
+            thr[c * 3 + b] = v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
+        }
+}
+
+/* Index (0..3) of the base drawn by the 32-bit uniform u. */
+static inline int markov_draw32(uint32_t u, const uint32_t *t) {
+    return (u >= t[0]) + (u >= t[1]) + (u >= t[2]);
+}
+
 typedef struct {
     uint64_t n_bases;   /* positions emitted by the Markov chain */
     uint64_t n_nrun;    /* positions inside N runs */
@@ -145,6 +159,8 @@ SYNTH_API void psacak_synth_genome(uint8_t *out, uint64_t n, uint64_t seed,
     xo_seed(&r, seed);
     double cum[64 * 4];
     markov_table(&r, cum, 64);
+    uint32_t thr[64 * 3];
+    markov_thresholds(cum, thr, 64);
     psacak_synth_genome_stats s;
     memset(&s, 0, sizeof(s));
     uint64_t p = 0;
@@ -166,13 +182,12 @@ SYNTH_API void psacak_synth_genome(uint8_t *out, uint64_t n, uint64_t seed,
             if (len > p) len = p;
             if (len > n - p) len = n - p;
             uint64_t src = xo_below(&r, p - len + 1);
-            for (uint64_t t = 0; t < len; t++) {
-                uint8_t c = out[src + t];
-                if (xo_unit(&r) < 0.01) {
-                    c = ACGT[xo_below(&r, 4)];
-                    s.n_mutated++;
-                }
-                out[p + t] = c;
+            memmove(out + p, out + src, len);
+            /* point mutations: each copied base with probability 0.01,
+               drawn as geometric gaps between mutated bases */
+            for (uint64_t t = xo_geometric(&r, 100.0) - 1; t < len; t += xo_geometric(&r, 100.0)) {
+                out[p + t] = ACGT[xo_below(&r, 4)];
+                s.n_mutated++;
             }
             p += len;
             s.n_copied += len;
@@ -182,10 +197,16 @@ SYNTH_API void psacak_synth_genome(uint8_t *out, uint64_t n, uint64_t seed,
         }
         uint64_t len = xo_geometric(&r, 2000.0);
         if (len > n - p) len = n - p;
-        for (uint64_t t = 0; t < len; t++) {
-            uint8_t c = markov_draw(&r, cum + ctx * 4);
-            out[p + t] = c;
-            ctx = ((ctx << 2) | base_code(c)) & 63;
+        for (uint64_t t = 0; t < len; t += 2) {
+            uint64_t x = xo_next(&r);
+            int b = markov_draw32((uint32_t)(x >> 32), thr + ctx * 3);
+            out[p + t] = ACGT[b];
+            ctx = ((ctx << 2) | b) & 63;
+            if (t + 1 < len) {
+                b = markov_draw32((uint32_t)x, thr + ctx * 3);
+                out[p + t + 1] = ACGT[b];
+                ctx = ((ctx << 2) | b) & 63;
+            }
         }
         p += len;
         s.n_bases += len;
@@ -194,16 +215,25 @@ SYNTH_API void psacak_synth_genome(uint8_t *out, uint64_t n, uint64_t seed,
 }
 
 /* Order-2 Markov chain over ACGT, transition rows drawn from the seed. */
+
 SYNTH_API void psacak_synth_markov2(uint8_t *out, uint64_t n, uint64_t seed) {
     xo_t r;
     xo_seed(&r, seed);
     double cum[16 * 4];
     markov_table(&r, cum, 16);
+    uint32_t thr[16 * 3];
+    markov_thresholds(cum, thr, 16);
     int ctx = 0;
-    for (uint64_t i = 0; i < n; i++) {
-        uint8_t c = markov_draw(&r, cum + ctx * 4);
-        out[i] = c;
-        ctx = ((ctx << 2) | base_code(c)) & 15;
+    for (uint64_t i = 0; i < n; i += 2) {
+        uint64_t x = xo_next(&r);
+        int b = markov_draw32((uint32_t)(x >> 32), thr + ctx * 3);
+        out[i] = ACGT[b];
+        ctx = ((ctx << 2) | b) & 15;
+        if (i + 1 < n) {
+            b = markov_draw32((uint32_t)x, thr + ctx * 3);
+            out[i + 1] = ACGT[b];
+            ctx = ((ctx << 2) | b) & 15;
+        }
     }
 }
 
