@@ -1,6 +1,7 @@
 // api.cu -- level recursion (the reference's psacak8 / psacak32 drivers) and
 // the C ABI of include/psacak_b200.h.
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <memory>
@@ -133,6 +134,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
         PSK_TRY(hist.init(ctx, 1));
         PSK_TRY(dgeom.init(ctx, 1));
     }
+    ctx.mark("enter", level);
     PSK_TRY(type_text<C>(text, n, types, lms, wcnt, bytes ? hist.get() : nullptr, tscratch, ctx.scan_ctas, s));
     tscratch.reset();
     PSK_TRY(lms_prefix(wcnt, nwords, pref, ctx.d_partial, ctx.d_scalars, ctx.scan_ctas, s));
@@ -177,6 +179,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
         PSK_CUDA(cudaMemsetAsync(cursor.get(), 0, n * sizeof(uint32_t), s));
     }
     const int engine = engine_for(ctx, level, bytes);
+    ctx.mark("typing+geometry", level);
 
     // Stage 1: sort the LMS substrings.
     if constexpr (sizeof(C) == 1) {
@@ -190,6 +193,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
                                    s));
     }
     cursor.reset();
+    ctx.mark("induce lms-substrings", level);
 
     // Stage 2: name them and build the reduced string.
     DBuf<uint32_t> sorted, red, heads, flags, sa1;
@@ -212,6 +216,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
     }
     sorted.reset();
     flags.reset();
+    ctx.mark("extract+name", level);
     PSK_TRY(sa1.init(ctx, n1));
     if (n1 > 0) {
         if (k < n1) {
@@ -236,7 +241,9 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
             uint64_t hsh = 0;
             PSK_TRY(hash_device(ctx, red, n1, &hsh));
             trace_push(ctx, level, width, n, n1, k, hsh);
+            ctx.mark("translate", level);
             PSK_TRY(build_level<uint32_t>(ctx, red, n1, sa1, level + 1));
+            ctx.mark("(back from recursion)", level);
         } else {
             heads.reset();
             if (level == 0 && ctx.debug_red) {
@@ -261,6 +268,7 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
         trace_push(ctx, level, width, n, 0, 0, 0);
     }
     red.reset();
+    ctx.mark("permute", level);
 
     // Stage 3: induce the whole suffix array from the sorted LMS suffixes.
     if constexpr (sizeof(C) == 1) {
@@ -341,7 +349,7 @@ status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
     int in1 = 0;
-    PSK_TRY((radix_sort_pairs<uint32_t, uint32_t>(k0, v0, k1, v1, n, 0, 32, ctx.d_hist, &in1, ctx.radix_ctas, s)));
+    PSK_TRY((ctx.radix_sort<uint32_t, uint32_t>(k0, v0, k1, v1, n, 0, 32, &in1)));
     const uint32_t *vals = in1 ? k1.get() : k0.get();
     const uint32_t *pos = in1 ? v1.get() : v0.get();
     PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(DistinctLoad{vals}, NoStore{}, n, ctx.d_partial, ctx.d_scalars + 3,
@@ -395,6 +403,8 @@ status_t ctx_init(Ctx &c, int device) {
     uint64_t thresh = UINT64_MAX;
     PSK_CUDA(cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh));
     PSK_CUDA(cudaMallocHost(&c.h_pinned, 4096));
+    PSK_CUDA(cudaMallocHost(&c.h_hist, RADIX_MAX_PASSES * 256 * sizeof(uint32_t)));
+    PSK_CUDA(cudaMalloc(&c.os.tickets, 64 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_partial, MAX_CHUNKS * 4 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_hist, 256 * RADIX_MAX_CTAS * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
@@ -411,6 +421,12 @@ status_t ctx_init(Ctx &c, int device) {
 
 void ctx_free(Ctx &c) {
     if (c.h_pinned) cudaFreeHost(c.h_pinned);
+    if (c.h_hist) cudaFreeHost(c.h_hist);
+    if (c.os.tickets) cudaFree(c.os.tickets);
+    if (c.os.status) cudaFree(c.os.status);
+    c.os.status = nullptr;
+    c.os.tickets = nullptr;
+    c.h_hist = nullptr;
     if (c.d_partial) cudaFree(c.d_partial);
     if (c.d_hist) cudaFree(c.d_hist);
     if (c.d_scalars) cudaFree(c.d_scalars);
@@ -438,7 +454,7 @@ struct ProfGuard {
 };
 
 // Folds the device-side count of entries scattered by the bucket scans into
-// the "induce_down" class (4 bytes read + 4 bytes written per entry).
+// the "induce_scatter" class (4 bytes read + 4 bytes written per entry).
 static status_t profile_collect(Ctx &c) {
     if (!c.profiling) return PSACAK_OK;
     c.prof.resolve();
@@ -447,7 +463,7 @@ static status_t profile_collect(Ctx &c) {
     PSK_CUDA(cudaMemsetAsync(c.d_induced, 0, sizeof(unsigned long long), c.stream));
     unsigned long long induced = ((unsigned long long)h[1] << 32) | h[0];
     if (induced) {
-        int cls = c.prof.cls_of("induce_down");
+        int cls = c.prof.cls_of("induce_scatter");
         c.prof.stats[cls].bytes += 8ull * induced;
     }
     return PSACAK_OK;
@@ -460,6 +476,11 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     c.stream = stream ? stream : c.own_stream;
     apply_schedule(c, sched);
     c.trace.clear();
+    {
+        const char *e = getenv("PSACAK_STAGE_TIMES");
+        c.stage_timing = e && e[0] == '1';
+        c.stage_t0 = 0;
+    }
     ProfGuard pg(c);
     status_t st;
     if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, n, d_sa, 0);
@@ -468,6 +489,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
         cudaStreamSynchronize(c.stream);
         return st;
     }
+    c.mark("final induce (level 0)", 0);
     PSK_TRY(c.sync());
     PSK_TRY(c.check_device_error());
     PSK_TRY(profile_collect(c));
@@ -728,7 +750,7 @@ static int debug_sort(psacak_ctx *ctx, K *keys, uint32_t *vals, uint64_t n, int 
     PSK_TRY(k1.init(c, n));
     PSK_TRY(v1.init(c, n));
     int in1 = 0;
-    PSK_TRY((radix_sort_pairs<K, uint32_t>(keys, vals, k1, v1, n, b0, b1, c.d_hist, &in1, c.radix_ctas, c.stream)));
+    PSK_TRY((c.radix_sort<K, uint32_t>(keys, vals, k1, v1, n, b0, b1, &in1)));
     if (in1) {
         PSK_CUDA(cudaMemcpyAsync(keys, k1.get(), n * sizeof(K), cudaMemcpyDeviceToDevice, c.stream));
         PSK_CUDA(cudaMemcpyAsync(vals, v1.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));

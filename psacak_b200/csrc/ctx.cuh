@@ -2,10 +2,13 @@
 // scratch for the primitives, the per-level trace.
 #pragma once
 
+#include <stdio.h>
+#include <time.h>
+
 #include <mutex>
 #include <vector>
 
-#include "prims.cuh"
+#include "radix.cuh"
 
 struct psacak_ctx;
 
@@ -21,6 +24,8 @@ struct Ctx {
     uint32_t *d_hist = nullptr;     // 256 * RADIX_MAX_CTAS radix histograms
     uint32_t *d_scalars = nullptr;  // 64 device scalars
     uint32_t *d_err = nullptr;      // device error word
+    uint32_t *h_hist = nullptr;     // pinned copy of the radix digit counts
+    OnesweepScratch os;             // look-back status words of the onesweep kernels
     uint32_t scan_ctas = 0;         // CTAs of the chunked scans
     uint32_t radix_ctas = 0;        // CTAs of the radix passes
     psacak_schedule sched{};
@@ -30,6 +35,8 @@ struct Ctx {
     uint64_t debug_cap = 0, debug_n1 = 0, debug_k = 0;
     std::vector<psacak_level_info> trace;
     bool profiling = false;
+    bool stage_timing = false;  // PSACAK_STAGE_TIMES=1: sync + print wall time per stage
+    double stage_t0 = 0;
     Profiler prof;
     unsigned long long *d_induced = nullptr;  // entries scattered by the bucket scans
     std::mutex mu;
@@ -57,6 +64,37 @@ struct Ctx {
         PSK_CUDA(cudaStreamSynchronize(stream));
         for (size_t i = 0; i < count; i++) h[i] = h_pinned[i];
         return PSACAK_OK;
+    }
+    // Debug aid: when stage timing is on, waits for the stream and prints the
+    // wall time since the previous mark.
+    void mark(const char *what, uint32_t level) {
+        if (!stage_timing) return;
+        cudaStreamSynchronize(stream);
+        struct timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        double t = ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+        if (stage_t0 > 0) fprintf(stderr, "[psacak] level %u %-24s %9.3f ms\n", level, what, t - stage_t0);
+        stage_t0 = t;
+    }
+    // Grows the onesweep status array to hold `tiles` tiles.
+    status_t ensure_onesweep(uint64_t tiles) {
+        if (tiles <= os.max_tiles) return PSACAK_OK;
+        uint64_t want = tiles + tiles / 4 + 64;
+        if (os.status) cudaFreeAsync(os.status, stream);
+        os.status = nullptr;
+        os.max_tiles = 0;
+        PSK_CUDA(cudaMallocAsync(&os.status, want * 256 * sizeof(uint64_t), stream));
+        // zeroed words read as "not ready" for every epoch
+        PSK_CUDA(cudaMemsetAsync(os.status, 0, want * 256 * sizeof(uint64_t), stream));
+        os.max_tiles = want;
+        return PSACAK_OK;
+    }
+    // Stable LSD radix sort of (key, value) pairs on bits [b0, b1); the
+    // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).
+    template <class K, class V>
+    status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1) {
+        PSK_TRY(ensure_onesweep(ceil_div(n, 3072) + 1));
+        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream);
     }
     status_t sync() {
         PSK_CUDA(cudaStreamSynchronize(stream));

@@ -28,6 +28,8 @@
 #include "ctx.cuh"
 #include "induce.cuh"
 
+#include <utility>
+
 namespace psk {
 
 constexpr int MS_BLOCK = 256;
@@ -49,17 +51,44 @@ struct BucketSeq {
 
 // ---- placement of the LMS positions --------------------------------------
 
-__global__ void k_place_lms_any8(const uint8_t *__restrict__ text, uint64_t nwords, const uint32_t *__restrict__ lms,
-                                 const ByteGeom *__restrict__ g, uint32_t *cursor, uint32_t *sa) {
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t word = lms[w];
-        while (word) {
-            int b = __ffs(word) - 1;
-            word &= word - 1;
-            uint64_t p = (w << 5) + b;
-            uint8_t c = text[p];
-            uint32_t slot = atomicAdd(&cursor[c], 1u);
-            sa[g->tail[c] - 1 - slot] = (uint32_t)p;
+// LMS-substring mode placement: LMS positions go to the tail of their bucket
+// in arbitrary order.  Each CTA walks a contiguous range of 32-position words
+// (a warp per word, a lane per position, so the text is read coalesced),
+// counts its LMS per character in shared memory, reserves one range per
+// character with a single global atomic, then writes into it.
+constexpr int PL_BLOCK = 256;
+__global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__restrict__ text, uint64_t nwords,
+                                                             const uint32_t *__restrict__ lms,
+                                                             const ByteGeom *__restrict__ g, uint32_t *cursor,
+                                                             uint32_t *sa, uint64_t wchunk) {
+    __shared__ uint32_t s_cnt[256], s_base[256];
+    s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, lt = lanemask_lt();
+    const uint64_t w0 = (uint64_t)blockIdx.x * wchunk;
+    const uint64_t w1 = w0 + wchunk < nwords ? w0 + wchunk : nwords;
+    for (int pass = 0; pass < 2; pass++) {
+        for (uint64_t w = w0 + warp; w < w1; w += PL_BLOCK / 32) {
+            uint32_t word = lms[w];
+            if (!word) continue;
+            bool on = (word >> lane) & 1u;
+            uint32_t c = on ? text[(w << 5) + lane] : 256u;
+            uint32_t peers = __match_any_sync(FULL_MASK, c);
+            int leader = __ffs(peers) - 1;
+            uint32_t got = 0;
+            if (on && (int)lane == leader) got = atomicAdd(&s_cnt[c], __popc(peers));
+            got = __shfl_sync(FULL_MASK, got, leader);
+            if (pass == 1 && on) {
+                uint32_t slot = s_base[c] + got + __popc(peers & lt);
+                sa[g->tail[c] - 1 - slot] = (uint32_t)((w << 5) + lane);
+            }
+        }
+        __syncthreads();
+        if (pass == 0) {
+            uint32_t c = threadIdx.x;
+            s_base[c] = s_cnt[c] ? atomicAdd(&cursor[c], s_cnt[c]) : 0u;
+            s_cnt[c] = 0;
+            __syncthreads();
         }
     }
 }
@@ -140,142 +169,45 @@ __global__ void k_place_cells(const uint32_t *__restrict__ vals, uint32_t ncells
 
 // ---- multisplit ----------------------------------------------------------
 
-// Per-CTA digit histogram of the entries that induce; the digit (the
-// predecessor's character) is kept in `dg` for the scatter pass.
-template <bool LSCAN>
-__global__ void __launch_bounds__(MS_BLOCK) k_ms_up(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sa,
-                                                    BucketSeq seq, uint32_t nitems, uint8_t c, uint64_t chunk,
-                                                    uint8_t *dg, uint32_t *hist, uint32_t G) {
-    __shared__ uint32_t sh[MS_WARPS][256];
-    for (int i = threadIdx.x; i < MS_WARPS * 256; i += MS_BLOCK) (&sh[0][0])[i] = 0;
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    uint64_t start = (uint64_t)blockIdx.x * chunk;
-    uint64_t end = start + chunk < nitems ? start + chunk : nitems;
-    const uint32_t invalid = LSCAN ? 0u : 255u;
-    for (uint64_t base = start; base < end; base += MS_BLOCK) {
-        uint64_t q = base + threadIdx.x;
-        uint32_t d = 256;
-        if (q < end) {
-            uint32_t x = sa[seq.slot((uint32_t)q)];
-            uint32_t dd = invalid;
-            if (x > 0) {
-                uint32_t c0 = text[x - 1];
-                if (LSCAN ? c0 > c : c0 < c) dd = c0;
-            }
-            dg[q] = (uint8_t)dd;
-            if (dd != invalid) d = dd;
-        }
-        uint32_t peers = __match_any_sync(FULL_MASK, d);
-        if (d < 256 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&sh[w][d], __popc(peers));
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += MS_BLOCK) {
-        uint32_t s = 0;
-        for (int ww = 0; ww < MS_WARPS; ww++) s += sh[ww][d];
-        hist[(uint64_t)d * G + blockIdx.x] = s;
-    }
-}
-
-// Turns the histograms into per-CTA start slots and advances the cursors.
-__global__ void k_ms_offsets(uint32_t *hist, uint32_t G, uint32_t *cursor, int dir, unsigned long long *induced) {
-    int d = threadIdx.x;
-    uint32_t run = cursor[d], tot = 0;
-    for (uint32_t b = 0; b < G; b++) {
-        uint32_t h = hist[(uint64_t)d * G + b];
-        hist[(uint64_t)d * G + b] = run;
-        run = dir > 0 ? run + h : run - h;
-        tot += h;
-    }
-    cursor[d] = run;
-    if (tot) atomicAdd(induced, (unsigned long long)tot);
-}
-
-template <bool LSCAN>
-__global__ void __launch_bounds__(MS_BLOCK) k_ms_down(const uint32_t *__restrict__ sa_in, BucketSeq seq,
-                                                      uint32_t nitems, uint64_t chunk, const uint8_t *__restrict__ dg,
-                                                      const uint32_t *__restrict__ hist, uint32_t G, uint32_t *sa_out,
-                                                      uint64_t n, uint32_t *err) {
-    __shared__ uint32_t s_val[MS_TILE];
-    __shared__ uint8_t s_dig[MS_TILE];
-    __shared__ uint32_t s_off[256];
-    __shared__ uint32_t s_tstart[256];
-    __shared__ uint32_t s_tcount[256];
-    __shared__ uint16_t s_wcnt[MS_WARPS][256];
-    __shared__ uint32_t s_scan[33];
-    const int w = threadIdx.x >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t lt = lanemask_lt();
-    const uint32_t invalid = LSCAN ? 0u : 255u;
-    uint64_t start = (uint64_t)blockIdx.x * chunk;
-    uint64_t end = start + chunk < nitems ? start + chunk : nitems;
-    s_off[threadIdx.x] = hist[(uint64_t)threadIdx.x * G + blockIdx.x];
-    for (uint64_t base = start; base < end; base += MS_TILE) {
-        for (int i = threadIdx.x; i < MS_WARPS * 256; i += MS_BLOCK) (&s_wcnt[0][0])[i] = 0;
-        __syncthreads();
-        uint32_t v[MS_IPT];
-        uint16_t rk[MS_IPT];
-        uint32_t dgt[MS_IPT];
-#pragma unroll
-        for (int r = 0; r < MS_IPT; r++) {
-            uint64_t q = base + (uint64_t)w * 32 * MS_IPT + (uint64_t)r * 32 + lane;
-            uint32_t d = 256;
-            if (q < end) {
-                uint32_t dd = dg[q];
-                if (dd != invalid) {
-                    d = dd;
-                    v[r] = sa_in[seq.slot((uint32_t)q)] - 1;
-                }
-            }
-            dgt[r] = d;
-            uint32_t peers = __match_any_sync(FULL_MASK, d);
-            uint32_t prior = d < 256 ? s_wcnt[w][d] : 0;
-            rk[r] = (uint16_t)(prior + __popc(peers & lt));
-            __syncwarp();
-            if (d < 256 && (int)lane == __ffs(peers) - 1) s_wcnt[w][d] = (uint16_t)(prior + __popc(peers));
-            __syncwarp();
-        }
-        __syncthreads();
-        {
-            uint32_t d = threadIdx.x, sum = 0;
-#pragma unroll
-            for (int ww = 0; ww < MS_WARPS; ww++) {
-                uint32_t cc = s_wcnt[ww][d];
-                s_wcnt[ww][d] = (uint16_t)sum;
-                sum += cc;
-            }
-            s_tcount[d] = sum;
-            uint32_t ex, tot;
-            block_scan<uint32_t, OpSum<uint32_t>, MS_BLOCK>(sum, OpSum<uint32_t>(), s_scan, &ex, &tot);
-            s_tstart[d] = ex;
-            if (d == 0) s_scan[32] = tot;
-        }
-        __syncthreads();
-        const uint32_t tile_valid = s_scan[32];
-#pragma unroll
-        for (int r = 0; r < MS_IPT; r++) {
-            if (dgt[r] < 256) {
-                uint32_t pos = s_tstart[dgt[r]] + s_wcnt[w][dgt[r]] + rk[r];
-                s_val[pos] = v[r];
-                s_dig[pos] = (uint8_t)dgt[r];
+// The bucket's entries in scan order; an entry x induces its predecessor
+// x-1 when that character c0 = text[x-1] is larger (L scan) or smaller (S
+// scan) than the bucket's character c, and the predecessor goes to slot
+// cur_in[c0] + rank (L) or cur_in[c0] - 1 - rank (S) -- the reference's
+// bucket-pointer increment/decrement, in scan order.
+template <bool LSCAN> struct BucketPolicy {
+    using Item = uint32_t;
+    const uint8_t *text;
+    uint32_t *sa;
+    BucketSeq seq;
+    uint32_t c;
+    const uint32_t *cur_in;
+    uint32_t *cur_out;
+    unsigned long long *induced;
+    uint64_t n;
+    uint32_t *err;
+    __device__ __forceinline__ void load(uint64_t i, Item &it, uint32_t &d) const {
+        uint32_t x = sa[seq.slot((uint32_t)i)];
+        d = 256;
+        if (x > 0) {
+            uint32_t c0 = text[x - 1];
+            if (LSCAN ? c0 > c : c0 < c) {
+                d = c0;
+                it = x - 1;
             }
         }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < tile_valid; i += MS_BLOCK) {
-            uint32_t d = s_dig[i];
-            uint32_t rank = i - s_tstart[d];
-            uint64_t o = LSCAN ? (uint64_t)s_off[d] + rank : (uint64_t)s_off[d] - 1 - rank;
-            if (o < n) sa_out[o] = s_val[i];
-            else dev_fail(err, DEVERR_RANGE);
-        }
-        __syncthreads();
-        {
-            uint32_t d = threadIdx.x;
-            s_off[d] = LSCAN ? s_off[d] + s_tcount[d] : s_off[d] - s_tcount[d];
-        }
-        __syncthreads();
     }
-}
+    __device__ __forceinline__ uint64_t out(uint32_t d, uint64_t r) const {
+        return LSCAN ? (uint64_t)cur_in[d] + r : (uint64_t)cur_in[d] - 1 - r;
+    }
+    __device__ __forceinline__ void store(uint64_t idx, const Item &it) const {
+        if (idx < n) sa[idx] = it;
+        else dev_fail(err, DEVERR_RANGE);
+    }
+    __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
+        cur_out[d] = LSCAN ? cur_in[d] + total : cur_in[d] - total;
+        if (total) atomicAdd(induced, (unsigned long long)total);
+    }
+};
 
 static inline uint32_t grid_cap(uint64_t n, uint32_t cap) {
     uint64_t g = ceil_div(n ? n : 1, 256);
@@ -308,8 +240,7 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
                     (k_expand_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, ncells, k0, v0)));
     PSK_LAUNCH_CHECK();
     int in1 = 0;
-    PSK_TRY((radix_sort_pairs<uint32_t, uint32_t>(k0, v0, k1, v1, ncells, 0, bitlen(maxrun), ctx.d_hist, &in1,
-                                                  ctx.radix_ctas, s)));
+    PSK_TRY((ctx.radix_sort<uint32_t, uint32_t>(k0, v0, k1, v1, ncells, 0, bitlen(maxrun), &in1)));
     uint32_t first = dir > 0 ? start + nseeds : start - nseeds;
     PSK_PROF_LAUNCH(s, "chain_place", ncells, 8ull * ncells,
                     (k_place_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(in1 ? v1 : v0, ncells, first, dir, sa)));
@@ -317,26 +248,21 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     return PSACAK_OK;
 }
 
+// Multisplit of one bucket; the cursors move from cur[0..256) to
+// cur[256..512) (the caller swaps the halves afterwards).
 template <bool LSCAN>
 static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t n, BucketSeq seq, uint8_t c,
-                           uint32_t *cursor, uint8_t *dg, cudaStream_t s) {
+                           const uint32_t *cur_in, uint32_t *cur_out, cudaStream_t s) {
     uint32_t nitems = seq.a_len + seq.b_len;
-    if (nitems == 0) return PSACAK_OK;
-    Chunking ch = make_chunking(nitems, MS_TILE, ctx.radix_ctas < RADIX_MAX_CTAS ? ctx.radix_ctas : RADIX_MAX_CTAS);
-    // algorithmic bytes: up reads each entry (4) and its predecessor's
-    // character (1) and writes the digit (1); down reads the digit (1) and,
-    // for inducing entries, the entry (4) and writes it to its bucket (4) --
-    // the inducing count is added from the device at the end of the build.
-    PSK_PROF_LAUNCH(s, "induce_up", nitems, 6ull * nitems,
-                    (k_ms_up<LSCAN><<<ch.G, MS_BLOCK, 0, s>>>(text, sa, seq, nitems, c, ch.chunk, dg, ctx.d_hist,
-                                                              ch.G)));
-    PSK_PROF_LAUNCH(s, "induce_offsets", 256, 0,
-                    (k_ms_offsets<<<1, 256, 0, s>>>(ctx.d_hist, ch.G, cursor, LSCAN ? 1 : -1, ctx.d_induced)));
-    PSK_PROF_LAUNCH(s, "induce_down", nitems, 1ull * nitems,
-                    (k_ms_down<LSCAN><<<ch.G, MS_BLOCK, 0, s>>>(sa, seq, nitems, ch.chunk, dg, ctx.d_hist, ch.G, sa, n,
-                                                                ctx.d_err)));
-    PSK_LAUNCH_CHECK();
-    return PSACAK_OK;
+    if (nitems == 0) {
+        PSK_CUDA(cudaMemcpyAsync(cur_out, cur_in, 256 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        return PSACAK_OK;
+    }
+    PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 4096) + 1));
+    BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err};
+    // algorithmic bytes: each entry read (4) and its predecessor's character
+    // (1); inducing entries written once (4, added from the device count).
+    return onesweep<BucketPolicy<LSCAN>, 16>(pol, nitems, ctx.os, ctx.d_err, s, "induce_scatter", 5ull * nitems);
 }
 
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms, const ByteGeom &hg,
@@ -349,24 +275,26 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         maxpart = hg.lcount[c] > maxpart ? hg.lcount[c] : maxpart;
         maxpart = hg.scount[c] > maxpart ? hg.scount[c] : maxpart;
     }
-    DBuf<uint32_t> cur, runs, off, k0, v0, k1, v1;
-    DBuf<uint8_t> dg;
+    DBuf<uint32_t> cur, cur2, runs, off, k0, v0, k1, v1;
     PSK_TRY(cur.init(ctx, 512));
+    PSK_TRY(cur2.init(ctx, 512));
     PSK_TRY(runs.init(ctx, maxpart));
     PSK_TRY(off.init(ctx, maxpart));
     PSK_TRY(k0.init(ctx, maxpart));
     PSK_TRY(v0.init(ctx, maxpart));
     PSK_TRY(k1.init(ctx, maxpart));
     PSK_TRY(v1.init(ctx, maxpart));
-    PSK_TRY(dg.init(ctx, maxbucket));
     uint32_t *curL = cur.get(), *curS = cur.get() + 256;
+    uint32_t *alt = cur2.get();
 
     // LMS positions at the bucket tails (put_lmscharacters / put_lmssuffixes).
     if (mode == INDUCE_LMS_SUBSTRINGS) {
         PSK_CUDA(cudaMemsetAsync(curL, 0, 256 * sizeof(uint32_t), s));
         const uint64_t nwords = ceil_div(n, 32);
+        const uint32_t G = ctx.scan_ctas;
+        const uint64_t wchunk = ceil_div(nwords, G);
         PSK_PROF_LAUNCH(s, "place_lms", nwords, 0,
-                        (k_place_lms_any8<<<grid_cap(nwords, 8192), 256, 0, s>>>(text, nwords, lms, dgeom, curL, sa)));
+                        (k_place_lms_any8<<<G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, wchunk)));
     } else if (n1 > 0) {
         PSK_PROF_LAUNCH(s, "place_lms", n1, 0,
                         (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(text, sorted_lms, n1, dgeom, sa)));
@@ -386,8 +314,10 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
             PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, runs, off, k0, v0, k1, v1, s));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
-        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, dg, s));
+        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, s));
+        std::swap(curL, alt);
     }
+    alt = cur2.get() + 256;
     // S scan: buckets in decreasing order, S parts filled from their tails.
     for (int c = 255; c >= 0; c--) {
         const uint32_t head = hg.head[c], tail = hg.tail[c];
@@ -400,7 +330,8 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
                                   s));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
-        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, dg, s));
+        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, s));
+        std::swap(curS, alt);
     }
     return PSACAK_OK;
 }

@@ -198,8 +198,7 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
                                                                                               k0, v0, ctx.d_err)));
         PSK_LAUNCH_CHECK();
         int in1 = 0;
-        PSK_TRY((radix_sort_pairs<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, ctx.d_hist, &in1,
-                                                      ctx.radix_ctas, s)));
+        PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, &in1)));
         const uint64_t *ks = in1 ? k1 : k0;
         const uint32_t *vs = in1 ? v1 : v0;
         PSK_TRY((chunk_scan<Tri, OpTri>(RoundLoad{ks, cnt, KB}, RoundStore{ks, vs, KB, R, sa, Wg, Wv, n, ctx.d_err}, cnt,

@@ -1,0 +1,190 @@
+// onesweep.cuh -- single-pass stable scatter by an 8-bit digit with
+// decoupled look-back.
+//
+// One kernel moves every item to its digit's output range, stable in input
+// order: each CTA claims the next tile (atomic ticket, so tiles are claimed
+// in order), ranks its items per digit in shared memory, publishes its
+// per-digit counts, and adds the counts of the tiles before it by walking
+// back until it meets a tile that already published an inclusive prefix.
+// The items are staged through shared memory in digit order so that the
+// writes leave in runs.
+//
+// Status words are 64-bit: [epoch:30 | flag:2 | count:32].  The epoch of a
+// launch is part of every word it writes, so words left by earlier launches
+// read as "not ready" and the array never needs clearing.  Every wait is
+// bounded: after SPIN_LIMIT polls the CTA records DEVERR_TIMEOUT and
+// proceeds (the build then fails with PSACAK_ETIMEOUT).  A predecessor tile
+// has always been claimed by a running or finished CTA, so the wait ends in
+// normal operation.
+//
+// A Policy supplies, per item index i < n:
+//   load(i, item, digit)            -> digit in [0, 256) or >= 256 to drop it
+//   out(digit, rank)                -> output index of the rank-th item of
+//                                      that digit (rank counts from 0 over all
+//                                      tiles of this launch)
+//   store(index, item)
+//   finish(digit, total)            -> called once per digit by the last tile
+#pragma once
+
+#include "prims.cuh"
+
+namespace psk {
+
+constexpr int OS_BLOCK = 256;
+constexpr int OS_WARPS = OS_BLOCK / 32;
+constexpr uint32_t OS_SPIN_LIMIT = 1u << 24;
+
+constexpr uint64_t OS_FLAG_AGG = 1ull;
+constexpr uint64_t OS_FLAG_PREFIX = 2ull;
+
+__device__ __forceinline__ uint64_t os_word(uint32_t epoch, uint64_t flag, uint32_t count) {
+    return ((uint64_t)epoch << 34) | (flag << 32) | count;
+}
+
+__device__ __forceinline__ uint64_t os_load(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void os_store(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+template <class Policy, int IPT>
+__global__ void __launch_bounds__(OS_BLOCK) k_onesweep(Policy pol, uint64_t n, uint64_t *status, uint32_t *ticket,
+                                                       uint32_t epoch, uint32_t ntiles, uint32_t *err) {
+    using Item = typename Policy::Item;
+    constexpr int TILE = OS_BLOCK * IPT;
+    extern __shared__ __align__(16) unsigned char os_smem[];
+    Item *s_item = (Item *)os_smem;
+    uint8_t *s_dig = (uint8_t *)(s_item + TILE);
+    __shared__ uint32_t s_excl[256];
+    __shared__ uint32_t s_tstart[256];
+    __shared__ uint32_t s_tcount[256];
+    __shared__ uint16_t s_wcnt[OS_WARPS][256];
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+
+    const int w = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    for (int i = threadIdx.x; i < OS_WARPS * 256; i += OS_BLOCK) (&s_wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * TILE;
+
+    // load every item of the thread first (independent loads in flight)
+    Item it[IPT];
+    uint32_t dg[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
+        dg[r] = 256;
+        if (i < n) pol.load(i, it[r], dg[r]);
+    }
+    // stable ranks within the warp's sub-tile
+    uint16_t rk[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        uint32_t d = dg[r] < 256 ? dg[r] : 256u;
+        uint32_t peers = __match_any_sync(FULL_MASK, d);
+        uint32_t prior = d < 256 ? s_wcnt[w][d] : 0u;
+        rk[r] = (uint16_t)(prior + __popc(peers & lt));
+        __syncwarp();
+        if (d < 256 && (int)lane == __ffs(peers) - 1) s_wcnt[w][d] = (uint16_t)(prior + __popc(peers));
+        __syncwarp();
+        dg[r] = d;
+    }
+    __syncthreads();
+    const uint32_t d = threadIdx.x;  // this thread's digit from here on
+    uint32_t count = 0;
+#pragma unroll
+    for (int ww = 0; ww < OS_WARPS; ww++) {
+        uint32_t c = s_wcnt[ww][d];
+        s_wcnt[ww][d] = (uint16_t)count;
+        count += c;
+    }
+    s_tcount[d] = count;
+    // publish, then look back
+    uint64_t *my = status + (uint64_t)tile * 256 + d;
+    if (tile == 0) {
+        os_store(my, os_word(epoch, OS_FLAG_PREFIX, count));
+        s_excl[d] = 0;
+    } else {
+        os_store(my, os_word(epoch, OS_FLAG_AGG, count));
+        uint32_t excl = 0;
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+            uint64_t v = os_load(status + (uint64_t)t * 256 + d);
+            uint32_t ep = (uint32_t)(v >> 34);
+            uint64_t fl = (v >> 32) & 3ull;
+            if (ep != epoch || fl == 0) {
+                if (++spins > OS_SPIN_LIMIT) {
+                    dev_fail(err, DEVERR_TIMEOUT);
+                    break;
+                }
+                continue;
+            }
+            excl += (uint32_t)v;
+            if (fl == OS_FLAG_PREFIX) break;
+            t--;
+        }
+        os_store(my, os_word(epoch, OS_FLAG_PREFIX, excl + count));
+        s_excl[d] = excl;
+    }
+    uint32_t ex, tot;
+    block_scan<uint32_t, OpSum<uint32_t>, OS_BLOCK>(count, OpSum<uint32_t>(), s_scan, &ex, &tot);
+    s_tstart[d] = ex;
+    if (tile == ntiles - 1) pol.finish(d, s_excl[d] + count);
+    __syncthreads();
+    // stage in digit order
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        if (dg[r] < 256) {
+            uint32_t pos = s_tstart[dg[r]] + s_wcnt[w][dg[r]] + rk[r];
+            s_item[pos] = it[r];
+            s_dig[pos] = (uint8_t)dg[r];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < tot; i += OS_BLOCK) {
+        uint32_t dd = s_dig[i];
+        uint64_t idx = pol.out(dd, (uint64_t)s_excl[dd] + (i - s_tstart[dd]));
+        pol.store(idx, s_item[i]);
+    }
+}
+
+// Scratch of one onesweep launch sequence: status words for `max_tiles`
+// tiles, a ticket per launch, and the launch epoch.
+struct OnesweepScratch {
+    uint64_t *status = nullptr;
+    uint32_t *tickets = nullptr;  // 64 tickets, reused round robin
+    uint64_t max_tiles = 0;
+    uint32_t epoch = 0;
+};
+
+template <class Policy, int IPT>
+status_t onesweep(Policy pol, uint64_t n, OnesweepScratch &sc, uint32_t *err, cudaStream_t s, const char *pname,
+                  uint64_t pbytes) {
+    if (n == 0) return PSACAK_OK;
+    constexpr int TILE = OS_BLOCK * IPT;
+    const uint64_t ntiles = ceil_div(n, TILE);
+    if (ntiles > sc.max_tiles) return set_error(PSACAK_EINTERNAL, "onesweep: %llu tiles exceed scratch", (unsigned long long)ntiles);
+    sc.epoch = (sc.epoch + 1) & ((1u << 30) - 1);
+    if (sc.epoch == 0) sc.epoch = 1;
+    uint32_t *ticket = sc.tickets + (sc.epoch & 63);
+    PSK_CUDA(cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s));
+    const size_t smem = (size_t)TILE * (sizeof(typename Policy::Item) + 1);
+    PSK_CUDA(cudaFuncSetAttribute(k_onesweep<Policy, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PSK_PROF_LAUNCH(s, pname, n, pbytes,
+                    (k_onesweep<Policy, IPT><<<(uint32_t)ntiles, OS_BLOCK, smem, s>>>(pol, n, sc.status, ticket,
+                                                                                      sc.epoch, (uint32_t)ntiles,
+                                                                                      err)));
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
+}  // namespace psk

@@ -4,7 +4,7 @@
 #include <stdio.h>
 #include <string.h>
 
-#include "prims.cuh"
+#include "radix.cuh"
 
 namespace psk {
 
@@ -31,20 +31,13 @@ status_t cuda_status(cudaError_t e, const char *what, const char *file, int line
 const char *last_error() { return t_last_error; }
 void clear_error() { t_last_error[0] = 0; }
 
-__global__ void __launch_bounds__(1024) k_radix_scan(uint32_t *hist, uint32_t total) {
+__global__ void k_radix_bases(const uint32_t *hist, uint32_t *bases) {
     __shared__ uint32_t smem[33];
-    uint32_t per = (total + 1023) / 1024;
-    uint32_t b = threadIdx.x * per;
-    uint32_t e = b + per < total ? b + per : total;
-    uint32_t s = 0;
-    for (uint32_t i = b; i < e; i++) s += hist[i];
+    const uint32_t p = blockIdx.x;
+    uint32_t v = hist[p * 256 + threadIdx.x];
     uint32_t ex;
-    block_scan<uint32_t, OpSum<uint32_t>, 1024>(s, OpSum<uint32_t>(), smem, &ex, (uint32_t *)nullptr);
-    for (uint32_t i = b; i < e; i++) {
-        uint32_t v = hist[i];
-        hist[i] = ex;
-        ex += v;
-    }
+    block_scan<uint32_t, OpSum<uint32_t>, 256>(v, OpSum<uint32_t>(), smem, &ex, (uint32_t *)nullptr);
+    bases[p * 256 + threadIdx.x] = ex;
 }
 
 }  // namespace psk

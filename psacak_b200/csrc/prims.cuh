@@ -191,159 +191,8 @@ status_t compact(Pred pred, Emit emit, uint64_t n, uint32_t *partial, uint32_t *
                                                  n, partial, count_out, OpSum<uint32_t>(), max_ctas, s);
 }
 
+// LSD radix sort of (key, value) pairs: see radix.cuh (single-pass scatter).
 // ---------------------------------------------------------------------------
-// LSD radix sort of (key, value) pairs, 8-bit digits.
-// ---------------------------------------------------------------------------
-constexpr int RADIX_BLOCK = 256;
-constexpr int RADIX_IPT = 16;
-constexpr int RADIX_TILE = RADIX_BLOCK * RADIX_IPT;
-constexpr int RADIX_WARPS = RADIX_BLOCK / 32;
 constexpr uint32_t RADIX_MAX_CTAS = 1024;
-
-template <class K>
-__global__ void __launch_bounds__(RADIX_BLOCK) k_radix_upsweep(const K *keys, uint64_t n, uint64_t chunk,
-                                                               int shift, uint32_t dmask, uint32_t *hist,
-                                                               uint32_t G) {
-    __shared__ uint32_t sh[RADIX_WARPS][256];
-    for (int i = threadIdx.x; i < RADIX_WARPS * 256; i += RADIX_BLOCK) (&sh[0][0])[i] = 0;
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    uint64_t start = (uint64_t)blockIdx.x * chunk;
-    uint64_t end = start + chunk < n ? start + chunk : n;
-    for (uint64_t base = start; base < end; base += RADIX_BLOCK) {
-        uint64_t i = base + threadIdx.x;
-        bool valid = i < end;
-        uint32_t d = valid ? ((uint32_t)(keys[i] >> shift) & dmask) : 256u;
-        uint32_t peers = __match_any_sync(FULL_MASK, d);
-        if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&sh[w][d], __popc(peers));
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += RADIX_BLOCK) {
-        uint32_t s = 0;
-        for (int ww = 0; ww < RADIX_WARPS; ww++) s += sh[ww][d];
-        hist[(uint64_t)d * G + blockIdx.x] = s;
-    }
-}
-
-// Exclusive scan over the digit-major [256][G] histogram in place.
-__global__ void __launch_bounds__(1024) k_radix_scan(uint32_t *hist, uint32_t total);
-
-template <class K, class V>
-__global__ void __launch_bounds__(RADIX_BLOCK) k_radix_downsweep(const K *__restrict__ kin, const V *__restrict__ vin,
-                                                                 K *__restrict__ kout, V *__restrict__ vout,
-                                                                 uint64_t n, uint64_t chunk, int shift, uint32_t dmask,
-                                                                 const uint32_t *__restrict__ hist, uint32_t G) {
-    extern __shared__ __align__(16) unsigned char radix_smem[];
-    K *skeys = (K *)radix_smem;
-    V *svals = (V *)(skeys + RADIX_TILE);
-    __shared__ uint32_t s_off[256];
-    __shared__ uint32_t s_tstart[256];
-    __shared__ uint32_t s_tcount[256];
-    __shared__ uint16_t s_wcnt[RADIX_WARPS][256];
-    __shared__ uint32_t s_scan[33];
-
-    const int w = threadIdx.x >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t lt = lanemask_lt();
-    uint64_t start = (uint64_t)blockIdx.x * chunk;
-    uint64_t end = start + chunk < n ? start + chunk : n;
-    for (int d = threadIdx.x; d < 256; d += RADIX_BLOCK) s_off[d] = hist[(uint64_t)d * G + blockIdx.x];
-
-    for (uint64_t base = start; base < end; base += RADIX_TILE) {
-        for (int i = threadIdx.x; i < RADIX_WARPS * 256; i += RADIX_BLOCK) (&s_wcnt[0][0])[i] = 0;
-        __syncthreads();
-        K k[RADIX_IPT];
-        V v[RADIX_IPT];
-        uint16_t rk[RADIX_IPT];
-        uint32_t dg[RADIX_IPT];
-#pragma unroll
-        for (int r = 0; r < RADIX_IPT; r++) {
-            uint64_t idx = base + (uint64_t)w * 32 * RADIX_IPT + (uint64_t)r * 32 + lane;
-            bool valid = idx < end;
-            if (valid) {
-                k[r] = kin[idx];
-                v[r] = vin[idx];
-            }
-            uint32_t d = valid ? ((uint32_t)(k[r] >> shift) & dmask) : 256u;
-            dg[r] = d;
-            uint32_t peers = __match_any_sync(FULL_MASK, d);
-            uint32_t prior = valid ? s_wcnt[w][d] : 0;
-            rk[r] = (uint16_t)(prior + __popc(peers & lt));
-            __syncwarp();
-            if (valid && (int)lane == __ffs(peers) - 1) s_wcnt[w][d] = (uint16_t)(prior + __popc(peers));
-            __syncwarp();
-        }
-        __syncthreads();
-        {
-            uint32_t d = threadIdx.x;
-            uint32_t sum = 0;
-#pragma unroll
-            for (int ww = 0; ww < RADIX_WARPS; ww++) {
-                uint32_t c = s_wcnt[ww][d];
-                s_wcnt[ww][d] = (uint16_t)sum;
-                sum += c;
-            }
-            s_tcount[d] = sum;
-            uint32_t ex;
-            block_scan<uint32_t, OpSum<uint32_t>, RADIX_BLOCK>(sum, OpSum<uint32_t>(), s_scan, &ex,
-                                                               (uint32_t *)nullptr);
-            s_tstart[d] = ex;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < RADIX_IPT; r++) {
-            if (dg[r] < 256) {
-                uint32_t pos = s_tstart[dg[r]] + s_wcnt[w][dg[r]] + rk[r];
-                skeys[pos] = k[r];
-                svals[pos] = v[r];
-            }
-        }
-        __syncthreads();
-        uint32_t tile_n = (uint32_t)((end - base) < (uint64_t)RADIX_TILE ? (end - base) : RADIX_TILE);
-        for (uint32_t i = threadIdx.x; i < tile_n; i += RADIX_BLOCK) {
-            K kk = skeys[i];
-            uint32_t d = (uint32_t)(kk >> shift) & dmask;
-            uint64_t o = (uint64_t)s_off[d] + (i - s_tstart[d]);
-            kout[o] = kk;
-            vout[o] = svals[i];
-        }
-        __syncthreads();
-        s_off[threadIdx.x] += s_tcount[threadIdx.x];
-        __syncthreads();
-    }
-}
-
-// Sorts n pairs by key bits [begin_bit, end_bit).  Ping-pongs between
-// (k0,v0) and (k1,v1); *result_in_1 tells where the sorted data ends up.
-// `hist` must hold 256 * RADIX_MAX_CTAS uint32.
-template <class K, class V>
-status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit, int end_bit,
-                          uint32_t *hist, int *result_in_1, uint32_t max_ctas, cudaStream_t s) {
-    *result_in_1 = 0;
-    if (n <= 1 || end_bit <= begin_bit) return PSACAK_OK;
-    Chunking c = make_chunking(n, RADIX_TILE, max_ctas < RADIX_MAX_CTAS ? max_ctas : RADIX_MAX_CTAS);
-    size_t smem = (size_t)RADIX_TILE * (sizeof(K) + sizeof(V));
-    PSK_CUDA(cudaFuncSetAttribute(k_radix_downsweep<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
-    K *ki = k0, *ko = k1;
-    V *vi = v0, *vo = v1;
-    int flip = 0;
-    for (int shift = begin_bit; shift < end_bit; shift += 8) {
-        int bits = end_bit - shift < 8 ? end_bit - shift : 8;
-        uint32_t dmask = (1u << bits) - 1;
-        PSK_PROF_LAUNCH(s, "radix_upsweep", n, n * sizeof(K),
-                        (k_radix_upsweep<K><<<c.G, RADIX_BLOCK, 0, s>>>(ki, n, c.chunk, shift, dmask, hist, c.G)));
-        PSK_PROF_LAUNCH(s, "radix_scan", 256 * c.G, 0, (k_radix_scan<<<1, 1024, 0, s>>>(hist, 256 * c.G)));
-        PSK_PROF_LAUNCH(s, "radix_downsweep", n, 2 * n * (sizeof(K) + sizeof(V)),
-                        (k_radix_downsweep<K, V><<<c.G, RADIX_BLOCK, smem, s>>>(ki, vi, ko, vo, n, c.chunk, shift,
-                                                                                 dmask, hist, c.G)));
-        PSK_LAUNCH_CHECK();
-        K *tk = ki; ki = ko; ko = tk;
-        V *tv = vi; vi = vo; vo = tv;
-        flip ^= 1;
-    }
-    *result_in_1 = flip;
-    return PSACAK_OK;
-}
 
 }  // namespace psk
