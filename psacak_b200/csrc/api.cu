@@ -111,7 +111,8 @@ static int engine_for(const Ctx &ctx, uint32_t level, bool bytes) {
 // the final induced sort.
 // ---------------------------------------------------------------------------
 template <class C>
-status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t level) {
+status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint32_t *bheads, uint64_t nbuckets,
+                     uint64_t n, uint32_t *sa, uint32_t level) {
     cudaStream_t s = ctx.stream;
     const uint32_t width = sizeof(C);
     if (n <= 3) {
@@ -175,6 +176,8 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
         PSK_KCOUNT();
         PSK_LAUNCH_CHECK();
         geom.scnt = scnt.get();
+        geom.names = names;
+        geom.heads = bheads;
         PSK_TRY(cursor.init(ctx, n));
         PSK_CUDA(cudaMemsetAsync(cursor.get(), 0, n * sizeof(uint32_t), s));
     }
@@ -186,22 +189,22 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
         if (engine == PSACAK_ENGINE_BUCKET)
             PSK_TRY(induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_LMS_SUBSTRINGS, nullptr, n1, sa, s));
         else
-            PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_LMS_SUBSTRINGS, nullptr, n1, cursor,
-                                       sa, s));
+            PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_LMS_SUBSTRINGS, nullptr, n1,
+                                       cursor, sa, s));
     } else {
-        PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_LMS_SUBSTRINGS, nullptr, n1, cursor, sa,
-                                   s));
+        PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, nbuckets, INDUCE_LMS_SUBSTRINGS, nullptr, n1,
+                                   cursor, sa, s));
     }
     cursor.reset();
     ctx.mark("induce lms-substrings", level);
 
     // Stage 2: name them and build the reduced string.
-    DBuf<uint32_t> sorted, red, heads, flags, sa1;
+    DBuf<uint32_t> sorted, red, heads, flags, sa1, names1;
     uint32_t k = 0;
     PSK_TRY(sorted.init(ctx, n1));
     if (n1 > 0) {
-        PSK_TRY(compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_partial, ctx.d_scalars + 1,
-                        ctx.scan_ctas, s));
+        PSK_TRY(ctx.compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_scalars + 1,
+                            "extract_lms"));
         uint32_t got = 0;
         PSK_TRY(ctx.read_u32(ctx.d_scalars + 1, &got));
         if (got != n1)
@@ -228,9 +231,11 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
                 PSK_TRY(c1.init(ctx, w1 + 1));
                 PSK_TRY(sc1.init(ctx, 2 * ceil_div(n1, TYPE_TILE) + 1024));
                 PSK_TRY(type_text<uint32_t>(red, n1, t1, l1, c1, nullptr, sc1, ctx.scan_ctas, s));
+                // the names stay as the next level's dense bucket ids
+                PSK_TRY(names1.init(ctx, n1));
+                PSK_CUDA(cudaMemcpyAsync(names1.get(), red.get(), n1 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
                 PSK_TRY(translate_names(red, n1, t1, heads, ctx.d_err, s));
             }
-            heads.reset();
             if (level == 0 && ctx.debug_red) {
                 uint64_t c = n1 < ctx.debug_cap ? n1 : ctx.debug_cap;
                 PSK_CUDA(cudaMemcpyAsync(ctx.debug_red, red.get(), c * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -242,7 +247,9 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
             PSK_TRY(hash_device(ctx, red, n1, &hsh));
             trace_push(ctx, level, width, n, n1, k, hsh);
             ctx.mark("translate", level);
-            PSK_TRY(build_level<uint32_t>(ctx, red, n1, sa1, level + 1));
+            // heads[c] (c <= k) are the next level's bucket boundaries by name
+            PSK_TRY(build_level<uint32_t>(ctx, red, names1, heads, k, n1, sa1, level + 1));
+            heads.reset();
             ctx.mark("(back from recursion)", level);
         } else {
             heads.reset();
@@ -268,15 +275,16 @@ status_t build_level(Ctx &ctx, const C *text, uint64_t n, uint32_t *sa, uint32_t
         trace_push(ctx, level, width, n, 0, 0, 0);
     }
     red.reset();
+    names1.reset();
     ctx.mark("permute", level);
 
     // Stage 3: induce the whole suffix array from the sorted LMS suffixes.
     if constexpr (sizeof(C) == 1) {
         if (engine == PSACAK_ENGINE_BUCKET)
             return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sa1, n1, sa, s);
-        return induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
+        return induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
     } else {
-        return induce_doubling<C>(ctx, text, n, types, lms, geom, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
+        return induce_doubling<C>(ctx, text, n, types, lms, geom, nbuckets, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
     }
 }
 
@@ -325,14 +333,35 @@ struct TailStore {
         out[p] = bm_get(types, p) ? tail - 1 : head[i];
     }
 };
+// index i starts a run of equal sorted symbols (i == n closes the last one)
+struct DistinctPred {
+    const uint32_t *vals;
+    uint64_t n;
+    __device__ __forceinline__ bool operator()(uint64_t i) const {
+        return i == n || i == 0 || vals[i] != vals[i - 1];
+    }
+};
+struct HeadEmit {
+    uint32_t *heads;
+    uint64_t n;
+    uint32_t distinct;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t slot) const {
+        if (slot <= distinct) heads[slot] = (uint32_t)i;
+    }
+};
 struct DistinctLoad {
     const uint32_t *vals;
     __device__ __forceinline__ uint32_t operator()(uint64_t i) const {
         return (i == 0 || vals[i] != vals[i - 1]) ? 1u : 0u;
     }
 };
-struct NoStore {
-    __device__ __forceinline__ void operator()(uint64_t, uint32_t, uint32_t) const {}
+// names[p] = rank of the symbol at p among the distinct symbols.
+struct RankStore {
+    const uint32_t *pos;
+    uint32_t *names;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t v) const {
+        names[pos[i]] = excl + v - 1;
+    }
 };
 
 status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa) {
@@ -352,8 +381,10 @@ status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa
     PSK_TRY((ctx.radix_sort<uint32_t, uint32_t>(k0, v0, k1, v1, n, 0, 32, &in1)));
     const uint32_t *vals = in1 ? k1.get() : k0.get();
     const uint32_t *pos = in1 ? v1.get() : v0.get();
-    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(DistinctLoad{vals}, NoStore{}, n, ctx.d_partial, ctx.d_scalars + 3,
-                                                   OpSum<uint32_t>(), ctx.scan_ctas, s)));
+    DBuf<uint32_t> names;
+    PSK_TRY(names.init(ctx, n));
+    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(DistinctLoad{vals}, RankStore{pos, names}, n, ctx.d_partial,
+                                                   ctx.d_scalars + 3, OpSum<uint32_t>(), ctx.scan_ctas, s)));
     uint32_t distinct = 0;
     PSK_TRY(ctx.read_u32(ctx.d_scalars + 3, &distinct));
     if (distinct >= n) {
@@ -387,7 +418,12 @@ status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa
     v0.reset();
     k1.reset();
     v1.reset();
-    return build_level<uint32_t>(ctx, t2, n, sa, 0);
+    // bucket boundaries by symbol rank
+    DBuf<uint32_t> bheads;
+    PSK_TRY(bheads.init(ctx, (uint64_t)distinct + 1));
+    PSK_TRY(compact(DistinctPred{vals, n}, HeadEmit{bheads, n, distinct}, n + 1, ctx.d_partial, (uint32_t *)nullptr,
+                    ctx.scan_ctas, s));
+    return build_level<uint32_t>(ctx, t2, names, bheads, distinct, n, sa, 0);
 }
 
 status_t ctx_init(Ctx &c, int device) {
@@ -432,6 +468,8 @@ void ctx_free(Ctx &c) {
     if (c.d_scalars) cudaFree(c.d_scalars);
     if (c.d_err) cudaFree(c.d_err);
     if (c.d_induced) cudaFree(c.d_induced);
+    if (c.arena) cudaFree(c.arena);
+    c.arena = nullptr;
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
     c.h_pinned = nullptr;
 }
@@ -476,6 +514,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     c.stream = stream ? stream : c.own_stream;
     apply_schedule(c, sched);
     c.trace.clear();
+    PSK_TRY(c.arena_prepare());
     {
         const char *e = getenv("PSACAK_STAGE_TIMES");
         c.stage_timing = e && e[0] == '1';
@@ -483,7 +522,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     }
     ProfGuard pg(c);
     status_t st;
-    if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, n, d_sa, 0);
+    if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, nullptr, nullptr, 256, n, d_sa, 0);
     else st = build_psacak32(c, d_text, n, d_sa);
     if (st != PSACAK_OK) {
         cudaStreamSynchronize(c.stream);
@@ -500,6 +539,7 @@ template <class C>
 status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_schedule *sched) {
     PSK_CUDA(cudaSetDevice(c.dev.id));
     c.stream = c.own_stream;
+    PSK_TRY(c.arena_prepare());
     DBuf<C> dt;
     DBuf<uint32_t> ds;
     PSK_TRY(dt.init(c, n));
@@ -823,7 +863,7 @@ int psacak_debug_reduced8(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, ui
     if (n > 3) {
         DBuf<uint32_t> sa;
         st = sa.init(c, n);
-        if (st == PSACAK_OK) st = build_level<uint8_t>(c, d_text, n, sa, 0);
+        if (st == PSACAK_OK) st = build_level<uint8_t>(c, d_text, nullptr, nullptr, 256, n, sa, 0);
     }
     c.debug_red = nullptr;
     if (st != PSACAK_OK) return st;

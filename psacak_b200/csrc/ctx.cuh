@@ -41,22 +41,78 @@ struct Ctx {
     unsigned long long *d_induced = nullptr;  // entries scattered by the bucket scans
     std::mutex mu;
 
+    // Workspace arena: one device buffer reused by every build.  Blocks are
+    // carved from the top and released stack-wise (a block freed out of
+    // order is reclaimed when everything above it is free).  A request that
+    // does not fit goes to the stream-ordered pool instead, and the arena is
+    // regrown to the observed high-water mark before the next build, so a
+    // steady workload allocates nothing after its first build.
+    struct Block {
+        void *ptr;
+        size_t size;
+        bool in_arena;
+        bool freed;
+    };
+    char *arena = nullptr;
+    size_t arena_size = 0, arena_top = 0, arena_vtop = 0, arena_high = 0;
+    std::vector<Block> blocks;
+
+    // Called at the start of a public call, when no block is live: regrows
+    // the arena to the high-water mark seen so far.
+    status_t arena_prepare() {
+        if (!blocks.empty()) return PSACAK_OK;
+        arena_top = arena_vtop = 0;
+        if (arena_high > arena_size) {
+            PSK_CUDA(cudaStreamSynchronize(stream));
+            if (arena) cudaFree(arena);
+            arena = nullptr;
+            arena_size = 0;
+            size_t want = arena_high + arena_high / 8 + (64u << 20);
+            PSK_CUDA(cudaMalloc(&arena, want));
+            arena_size = want;
+        }
+        return PSACAK_OK;
+    }
     template <class T>
     status_t alloc(T **p, size_t count) {
         size_t bytes = count * sizeof(T);
         if (bytes == 0) bytes = 16;
+        bytes = (bytes + 255) & ~(size_t)255;
+        arena_vtop += bytes;
+        if (arena_vtop > arena_high) arena_high = arena_vtop;
+        if (arena && arena_top + bytes <= arena_size) {
+            blocks.push_back(Block{arena + arena_top, bytes, true, false});
+            *p = (T *)(arena + arena_top);
+            arena_top += bytes;
+            return PSACAK_OK;
+        }
         void *q = nullptr;
         cudaError_t e = cudaMallocFromPoolAsync(&q, bytes, pool, stream);
         if (e != cudaSuccess) {
+            arena_vtop -= bytes;
             *p = nullptr;
             return set_error(PSACAK_ENOMEM, "device allocation of %zu bytes failed: %s", bytes,
                              cudaGetErrorString(e));
         }
+        blocks.push_back(Block{q, bytes, false, false});
         *p = (T *)q;
         return PSACAK_OK;
     }
     void release(void *p) {
-        if (p) cudaFreeAsync(p, stream);
+        if (!p) return;
+        for (size_t i = blocks.size(); i-- > 0;) {
+            if (blocks[i].ptr == p && !blocks[i].freed) {
+                blocks[i].freed = true;
+                if (!blocks[i].in_arena) cudaFreeAsync(p, stream);
+                break;
+            }
+        }
+        while (!blocks.empty() && blocks.back().freed) {
+            const Block &b = blocks.back();
+            arena_vtop -= b.size;
+            if (b.in_arena) arena_top = (size_t)((char *)b.ptr - arena);
+            blocks.pop_back();
+        }
     }
     // Copies `count` uint32 from device to host and waits for the stream.
     status_t read_u32(const uint32_t *d, uint32_t *h, size_t count = 1) {
@@ -93,8 +149,14 @@ struct Ctx {
     // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).
     template <class K, class V>
     status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1) {
-        PSK_TRY(ensure_onesweep(ceil_div(n, 3072) + 1));
+        PSK_TRY(ensure_onesweep(ceil_div(n, 12 * OS_BLOCK) + 1));
         return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream);
+    }
+    // Single-pass stable compaction (see compact1).
+    template <class Pred, class Emit>
+    status_t compact(Pred pred, Emit emit, uint64_t n, uint32_t *count_out, const char *name) {
+        PSK_TRY(ensure_onesweep(ceil_div(n, 12 * OS_BLOCK) + 1));
+        return compact1(pred, emit, n, count_out, os, d_err, stream, name);
     }
     status_t sync() {
         PSK_CUDA(cudaStreamSynchronize(stream));

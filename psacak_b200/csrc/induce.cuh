@@ -29,6 +29,10 @@ struct WordGeom {
 template <class C> struct Geom;
 template <> struct Geom<uint8_t> {
     const ByteGeom *g;
+    __device__ __forceinline__ uint32_t name(uint64_t, uint8_t c) const { return c; }
+    // first slot of the L (S) part of the bucket with dense id c
+    __device__ __forceinline__ uint32_t lstart_of(uint32_t c) const { return g->head[c]; }
+    __device__ __forceinline__ uint32_t sstart_of(uint32_t c) const { return g->tail[c] - g->scount[c]; }
     __device__ __forceinline__ uint32_t lgroup(uint8_t c) const { return g->head[c]; }
     __device__ __forceinline__ uint32_t sgroup(uint8_t c) const { return g->tail[c] - g->scount[c]; }
     __device__ __forceinline__ uint32_t tail(uint8_t c) const { return g->tail[c]; }
@@ -36,6 +40,14 @@ template <> struct Geom<uint8_t> {
 };
 template <> struct Geom<uint32_t> {
     const uint32_t *scnt;
+    const uint32_t *names;  // dense bucket id of every position
+    const uint32_t *heads;  // bucket boundaries by dense id (nbuckets + 1 entries)
+    __device__ __forceinline__ uint32_t name(uint64_t j, uint32_t) const { return names[j]; }
+    __device__ __forceinline__ uint32_t lstart_of(uint32_t c) const { return heads[c]; }
+    __device__ __forceinline__ uint32_t sstart_of(uint32_t c) const {
+        uint32_t tail = heads[c + 1];
+        return tail - scnt[tail - 1];
+    }
     __device__ __forceinline__ uint32_t lgroup(uint32_t v) const { return v; }
     __device__ __forceinline__ uint32_t sgroup(uint32_t v) const { return v + 1 - scnt[v]; }
     __device__ __forceinline__ uint32_t tail(uint32_t v) const { return v + 1; }
@@ -49,9 +61,10 @@ enum InduceMode { INDUCE_LMS_SUBSTRINGS = 0, INDUCE_FINAL = 1 };
 // mode `sorted_lms` (n1 entries, ascending suffix order) gives their order.
 // Writes every SA slot.  `cursor` is n (u32 levels) or 256 (byte levels)
 // zeroed uint32 used to place LMS positions in the first mode.
+// `nbuckets` = number of distinct symbols (dense ids 0..nbuckets-1).
 template <class C>
 status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
-                         Geom<C> geom, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
+                         Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
                          uint32_t *cursor, uint32_t *sa, cudaStream_t s);
 
 // Bucket-ordered induced sort of a byte level (the reference's induce scan

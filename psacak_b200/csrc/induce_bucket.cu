@@ -176,6 +176,7 @@ __global__ void k_place_cells(const uint32_t *__restrict__ vals, uint32_t ncells
 // bucket-pointer increment/decrement, in scan order.
 template <bool LSCAN> struct BucketPolicy {
     using Item = uint32_t;
+    static constexpr int kMinBlocks = 4;
     const uint8_t *text;
     uint32_t *sa;
     BucketSeq seq;
@@ -258,11 +259,11 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
         PSK_CUDA(cudaMemcpyAsync(cur_out, cur_in, 256 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         return PSACAK_OK;
     }
-    PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 4096) + 1));
+    PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 12 * OS_BLOCK) + 1));
     BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err};
     // algorithmic bytes: each entry read (4) and its predecessor's character
     // (1); inducing entries written once (4, added from the device count).
-    return onesweep<BucketPolicy<LSCAN>, 16>(pol, nitems, ctx.os, ctx.d_err, s, "induce_scatter", 5ull * nitems);
+    return onesweep<BucketPolicy<LSCAN>, 12>(pol, nitems, ctx.os, ctx.d_err, s, "induce_scatter", 5ull * nitems);
 }
 
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms, const ByteGeom &hg,

@@ -23,16 +23,21 @@
 #include "ctx.cuh"
 #include "induce.cuh"
 
+#include <utility>
+
 namespace psk {
 
+// Per sorted item: last group start (max), last subgroup start (max), kept
+// items (sum) and kept subgroups started (sum).
 struct Tri {
-    uint32_t g, s, k;
+    uint32_t g, s, k, o;
 };
 __device__ __forceinline__ Tri shfl_up_t(Tri v, int o) {
     Tri r;
     r.g = __shfl_up_sync(FULL_MASK, v.g, o);
     r.s = __shfl_up_sync(FULL_MASK, v.s, o);
     r.k = __shfl_up_sync(FULL_MASK, v.k, o);
+    r.o = __shfl_up_sync(FULL_MASK, v.o, o);
     return r;
 }
 struct OpTri {
@@ -41,9 +46,10 @@ struct OpTri {
         r.g = a.g > b.g ? a.g : b.g;
         r.s = a.s > b.s ? a.s : b.s;
         r.k = a.k + b.k;
+        r.o = a.o + b.o;
         return r;
     }
-    __device__ __forceinline__ static Tri identity() { return Tri{0, 0, 0}; }
+    __device__ __forceinline__ static Tri identity() { return Tri{0, 0, 0, 0}; }
 };
 
 // ---- terminal slots of the LMS positions ---------------------------------
@@ -103,6 +109,8 @@ template <class C, bool STYPE> struct WPred {
     const uint32_t *types;
     __device__ __forceinline__ bool operator()(uint64_t j) const { return bm_get(types, j) == STYPE; }
 };
+// Work item = (dense group id, position); the group id of round 1 is the
+// symbol's name and gstart[id] the first SA slot of its L (or S) part.
 template <class C, bool STYPE> struct WEmit {
     const C *text;
     Geom<C> g;
@@ -110,11 +118,17 @@ template <class C, bool STYPE> struct WEmit {
     __device__ __forceinline__ void operator()(uint64_t j, uint32_t slot) const {
         C c = text[j];
         uint32_t grp = STYPE ? g.sgroup(c) : g.lgroup(c);
-        Wg[slot] = grp;
+        Wg[slot] = g.name(j, c);
         Wv[slot] = (uint32_t)j;
         R[j] = grp + 1;
     }
 };
+
+template <class C, bool STYPE>
+__global__ void k_group_starts(Geom<C> g, uint64_t nbuckets, uint32_t *gstart) {
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nbuckets; c += (uint64_t)gridDim.x * blockDim.x)
+        gstart[c] = STYPE ? g.sstart_of((uint32_t)c) : g.lstart_of((uint32_t)c);
+}
 
 __global__ void k_keys(const uint32_t *__restrict__ Wg, const uint32_t *__restrict__ Wv, uint64_t cnt,
                        const uint32_t *__restrict__ R, uint64_t n, uint64_t h, int KB, uint64_t *keys,
@@ -146,7 +160,9 @@ struct RoundLoad {
         Tri t;
         t.g = gb ? (uint32_t)(i + 1) : 0u;
         t.s = sb ? (uint32_t)(i + 1) : 0u;
-        t.k = (sb && sbn) ? 0u : 1u;
+        bool keep = !(sb && sbn);
+        t.k = keep ? 1u : 0u;
+        t.o = (keep && sb) ? 1u : 0u;
         return t;
     }
 };
@@ -154,23 +170,31 @@ struct RoundStore {
     const uint64_t *keys;
     const uint32_t *vals;
     int KB;
+    const uint32_t *gstart;  // group id -> first slot (this round)
+    uint32_t *gnext;         // kept subgroup ordinal -> first slot (next round)
     uint32_t *R, *sa, *Wg, *Wv;
-    uint64_t n;
+    uint64_t n, ngroups;
     uint32_t *err;
     __device__ __forceinline__ void operator()(uint64_t i, Tri excl, Tri v) const {
         uint32_t gs = (excl.g > v.g ? excl.g : v.g) - 1;
         uint32_t ss = (excl.s > v.s ? excl.s : v.s) - 1;
-        uint32_t g = (uint32_t)(keys[i] >> KB);
-        uint32_t newg = g + (ss - gs);
+        uint64_t gid = keys[i] >> KB;
         uint32_t val = vals[i];
-        if (newg >= n || val >= n) {
+        if (gid >= ngroups || val >= n) {
+            dev_fail(err, DEVERR_RANGE);
+            return;
+        }
+        uint32_t newg = gstart[gid] + (ss - gs);
+        if (newg >= n) {
             dev_fail(err, DEVERR_RANGE);
             return;
         }
         R[val] = newg + 1;
         if (v.k) {
-            Wg[excl.k] = newg;
+            uint32_t ord = excl.o + v.o - 1;
+            Wg[excl.k] = ord;
             Wv[excl.k] = val;
+            if (v.o) gnext[ord] = newg;
         } else {
             sa[newg] = val;
         }
@@ -180,17 +204,23 @@ struct RoundStore {
 // One scan (L or S): resolves the chains of every item of the given type.
 template <class C, bool STYPE>
 static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, Geom<C> geom,
-                              uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0,
-                              uint64_t *k1, uint32_t *v1, cudaStream_t s) {
+                              uint64_t nbuckets, uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0,
+                              uint32_t *v0, uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, cudaStream_t s) {
     uint32_t *d_cnt = ctx.d_scalars;
-    PSK_TRY(compact(WPred<C, STYPE>{types}, WEmit<C, STYPE>{text, geom, Wg, Wv, R}, n, ctx.d_partial, d_cnt,
-                    ctx.scan_ctas, s));
+    {
+        uint64_t gb = ceil_div(nbuckets, 256);
+        k_group_starts<C, STYPE><<<(uint32_t)(gb < 4096 ? gb : 4096), 256, 0, s>>>(geom, nbuckets, gA);
+        PSK_KCOUNT();
+        PSK_LAUNCH_CHECK();
+    }
+    PSK_TRY(ctx.compact(WPred<C, STYPE>{types}, WEmit<C, STYPE>{text, geom, Wg, Wv, R}, n, d_cnt, "double_items"));
     uint32_t cnt = 0;
     PSK_TRY(ctx.read_u32(d_cnt, &cnt));
     const int KB = bitlen(n);
-    const int GB = bitlen(n - 1);
+    uint64_t ngroups = nbuckets;
     Tri *d_tri = (Tri *)(ctx.d_scalars + 4);
     for (uint64_t h = 1; cnt > 0; h <<= 1) {
+        const int GB = bitlen(ngroups > 0 ? ngroups - 1 : 0);
         if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
         uint64_t gblocks = ceil_div(cnt, 256);
         PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
@@ -201,21 +231,28 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
         PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, &in1)));
         const uint64_t *ks = in1 ? k1 : k0;
         const uint32_t *vs = in1 ? v1 : v0;
-        PSK_TRY((chunk_scan<Tri, OpTri>(RoundLoad{ks, cnt, KB}, RoundStore{ks, vs, KB, R, sa, Wg, Wv, n, ctx.d_err}, cnt,
+        PSK_TRY((chunk_scan<Tri, OpTri>(RoundLoad{ks, cnt, KB},
+                                        RoundStore{ks, vs, KB, gA, gB, R, sa, Wg, Wv, n, ngroups, ctx.d_err}, cnt,
                                         (Tri *)ctx.d_partial, d_tri, OpTri(), ctx.scan_ctas, s)));
-        uint32_t tri[3];
-        PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 3));
+        uint32_t tri[4];
+        PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
         cnt = tri[2];
+        ngroups = tri[3];
+        std::swap(gA, gB);
     }
     return PSACAK_OK;
 }
 
 template <class C>
 status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
-                         Geom<C> geom, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1, uint32_t *cursor,
-                         uint32_t *sa, cudaStream_t s) {
-    DBuf<uint32_t> R, Wg, Wv, v0, v1;
+                         Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
+                         uint32_t *cursor, uint32_t *sa, cudaStream_t s) {
+    DBuf<uint32_t> R, Wg, Wv, v0, v1, gA, gB;
     DBuf<uint64_t> k0, k1;
+    // group-start tables: indexed by bucket id (round 1) or kept-group ordinal
+    const uint64_t gcap = n > nbuckets ? n : nbuckets;
+    PSK_TRY(gA.init(ctx, gcap));
+    PSK_TRY(gB.init(ctx, gcap));
     PSK_TRY(R.init(ctx, n + 1));
     PSK_TRY(Wg.init(ctx, n));
     PSK_TRY(Wv.init(ctx, n));
@@ -237,16 +274,16 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
                                                        ctx.d_partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
                                                        ctx.scan_ctas, s)));
     }
-    PSK_TRY((doubling_scan<C, false>(ctx, text, n, types, geom, R, sa, Wg, Wv, k0, v0, k1, v1, s)));
-    PSK_TRY((doubling_scan<C, true>(ctx, text, n, types, geom, R, sa, Wg, Wv, k0, v0, k1, v1, s)));
+    PSK_TRY((doubling_scan<C, false>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));
+    PSK_TRY((doubling_scan<C, true>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));
     return PSACAK_OK;
 }
 
 template status_t induce_doubling<uint8_t>(Ctx &, const uint8_t *, uint64_t, const uint32_t *, const uint32_t *,
-                                           Geom<uint8_t>, InduceMode, const uint32_t *, uint64_t, uint32_t *,
+                                           Geom<uint8_t>, uint64_t, InduceMode, const uint32_t *, uint64_t, uint32_t *,
                                            uint32_t *, cudaStream_t);
 template status_t induce_doubling<uint32_t>(Ctx &, const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
-                                            Geom<uint32_t>, InduceMode, const uint32_t *, uint64_t, uint32_t *,
-                                            uint32_t *, cudaStream_t);
+                                            Geom<uint32_t>, uint64_t, InduceMode, const uint32_t *, uint64_t,
+                                            uint32_t *, uint32_t *, cudaStream_t);
 
 }  // namespace psk

@@ -24,6 +24,7 @@
 //                                      tiles of this launch)
 //   store(index, item)
 //   finish(digit, total)            -> called once per digit by the last tile
+//   kMinBlocks                      -> CTAs per SM the register budget must allow
 #pragma once
 
 #include "prims.cuh"
@@ -51,7 +52,7 @@ __device__ __forceinline__ void os_store(uint64_t *p, uint64_t v) {
 }
 
 template <class Policy, int IPT>
-__global__ void __launch_bounds__(OS_BLOCK) k_onesweep(Policy pol, uint64_t n, uint64_t *status, uint32_t *ticket,
+__global__ void __launch_bounds__(OS_BLOCK, Policy::kMinBlocks) k_onesweep(Policy pol, uint64_t n, uint64_t *status, uint32_t *ticket,
                                                        uint32_t epoch, uint32_t ntiles, uint32_t *err) {
     using Item = typename Policy::Item;
     constexpr int TILE = OS_BLOCK * IPT;
@@ -185,6 +186,43 @@ status_t onesweep(Policy pol, uint64_t n, OnesweepScratch &sc, uint32_t *err, cu
                                                                                       err)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
+}
+
+}  // namespace psk
+
+namespace psk {
+
+// Stable compaction through the same kernel: kept items carry digit 0.
+template <class Pred, class Emit> struct CompactPolicy {
+    using Item = uint32_t;
+    static constexpr int kMinBlocks = 4;
+    Pred pred;
+    Emit emit;
+    uint32_t *count;
+    __device__ __forceinline__ void load(uint64_t i, Item &it, uint32_t &d) const {
+        if (pred(i)) {
+            d = 0;
+            it = (uint32_t)i;
+        }
+    }
+    __device__ __forceinline__ uint64_t out(uint32_t, uint64_t r) const { return r; }
+    __device__ __forceinline__ void store(uint64_t idx, const Item &it) const { emit((uint64_t)it, (uint32_t)idx); }
+    __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
+        if (d == 0 && count) *count = total;
+    }
+};
+
+// Single-pass stable compaction: emit(i, slot) for every i < n with pred(i),
+// slots consecutive in index order; *count_out (device, nullable) = kept.
+template <class Pred, class Emit>
+status_t compact1(Pred pred, Emit emit, uint64_t n, uint32_t *count_out, OnesweepScratch &sc, uint32_t *err,
+                  cudaStream_t s, const char *pname) {
+    if (n == 0) {
+        if (count_out) PSK_CUDA(cudaMemsetAsync(count_out, 0, sizeof(uint32_t), s));
+        return PSACAK_OK;
+    }
+    return onesweep<CompactPolicy<Pred, Emit>, 12>(CompactPolicy<Pred, Emit>{pred, emit, count_out}, n, sc, err, s,
+                                                   pname, 0);
 }
 
 }  // namespace psk

@@ -20,6 +20,7 @@ template <class K, class V> struct RadixItem {
 
 template <class K, class V> struct RadixPolicy {
     using Item = RadixItem<K, V>;
+    static constexpr int kMinBlocks = sizeof(K) == 8 ? 3 : 4;
     const K *kin;
     const V *vin;
     K *kout;
@@ -101,7 +102,7 @@ status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit,
         int shift = begin_bit + 8 * p;
         int bits = end_bit - shift < 8 ? end_bit - shift : 8;
         RadixPolicy<K, V> pol{ki, vi, ko, vo, shift, (1u << bits) - 1, bases + p * 256};
-        constexpr int IPT = sizeof(K) == 8 ? 12 : 16;
+        constexpr int IPT = 12;
         PSK_TRY((onesweep<RadixPolicy<K, V>, IPT>(pol, n, sc, err, s, "radix_pass", 2 * n * (sizeof(K) + sizeof(V)))));
         K *tk = ki; ki = ko; ko = tk;
         V *tv = vi; vi = vo; vo = tv;
