@@ -289,8 +289,11 @@ def psacak_inplace(text, suf):
         raise ValueError("the suffix array is shorter than the text")
     if t.size >= 0xFFFFFFFF:
         raise ValueError("text length must be below 2**32 - 1")
-    out = _ctx().psacak(t)
-    suf[:t.size] = out
+    if suf.flags["C_CONTIGUOUS"]:
+        # write straight into the caller's buffer (only suf[:len(text)] changes)
+        _raise(lib().psacak8_ctx(_ctx().handle, _vp(t), t.size, _vp(suf), None))
+    else:
+        suf[:t.size] = _ctx().psacak(t)
 
 
 def psacak32(symbols):
