@@ -146,6 +146,26 @@ PSACAK_API int psacak_profile_enable(psacak_ctx *ctx, int on);
 PSACAK_API int psacak_profile_reset(psacak_ctx *ctx);
 PSACAK_API int psacak_profile_get(psacak_ctx *ctx, psacak_kernel_stat *out, uint32_t cap, uint32_t *count);
 
+/* Largest n accepted by psacak_check_sa8_noalloc (8 MiB of fixed scratch). */
+#define PSACAK_NOALLOC_CHECK_MAX (1u << 21)
+
+/*
+ * psacak_check_sa8_noalloc -- the check of psacak_check_sa8_dev for callers
+ * that cannot allocate device memory: a serving loop in which cudaMalloc /
+ * cudaFree would synchronise the device and stall its other streams, or a
+ * host process that owns the device memory budget and forbids allocations by
+ * its plugins.  No counterpart in the reference.  It allocates nothing: its
+ * scratch is an array of PSACAK_NOALLOC_CHECK_MAX entries compiled into the
+ * library (held on every GPU that loads the library until exit), so n above
+ * that limit returns PSACAK_EINVAL.  No context is used; `stream` is a
+ * cudaStream_t (NULL = default stream) on the current device.  The first call
+ * on a device looks up the array's device address and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race.  Returns after the check has finished on `stream`.
+ */
+PSACAK_API int psacak_check_sa8_noalloc(const uint8_t *d_text, uint64_t n, const uint32_t *d_sa, int *ok,
+                                        void *stream);
+
 /* Number of kernels the library launched since the context was created. */
 PSACAK_API uint64_t psacak_kernel_launches(psacak_ctx *ctx);
 

@@ -120,6 +120,8 @@ def lib():
         L.psacak_profile_enable.argtypes = [p, i32]
         L.psacak_profile_reset.argtypes = [p]
         L.psacak_profile_get.argtypes = [p, p, u32, ctypes.POINTER(u32)]
+        L.psacak_check_sa8_noalloc.argtypes = [p, u64, p, ctypes.POINTER(i32), p]
+        L.psacak_check_sa8_noalloc.restype = i32
         L.psacak_kernel_launches.argtypes = [p]
         L.psacak_kernel_launches.restype = u64
         for name in ("psacak8", "psacak32", "psacak8_ctx", "psacak32_ctx", "psacak8_dev", "psacak32_dev",
@@ -262,6 +264,19 @@ def _sched_ptr(schedule):
             setattr(s, k, int(v))
         schedule = s
     return ctypes.byref(schedule)
+
+
+NOALLOC_CHECK_MAX = 1 << 21
+
+
+def check_sa8_noalloc(d_text, n, d_sa, stream=0):
+    """Suffix-array check for callers that may not allocate device memory:
+    uses a fixed scratch array inside the library (n <= NOALLOC_CHECK_MAX);
+    calls overlapping on the GPU race.  Device pointers as ints."""
+    ok = ctypes.c_int(0)
+    _raise(lib().psacak_check_sa8_noalloc(ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa), ctypes.byref(ok),
+                                          ctypes.c_void_p(stream)))
+    return bool(ok.value)
 
 
 _default = threading.local()
