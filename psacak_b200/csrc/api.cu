@@ -185,12 +185,26 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     ctx.mark("typing+geometry", level);
 
     // Stage 1: sort the LMS substrings.
+    DBuf<uint32_t> sorted;
+    PSK_TRY(sorted.init(ctx, n1));
+    bool extracted = false;
     if constexpr (sizeof(C) == 1) {
-        if (engine == PSACAK_ENGINE_BUCKET)
-            PSK_TRY(induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_LMS_SUBSTRINGS, nullptr, n1, sa, s));
-        else
+        if (engine == PSACAK_ENGINE_BUCKET) {
+            unsigned long long *lmscnt = ctx.d_induced + 1;
+            PSK_CUDA(cudaMemsetAsync(lmscnt, 0, sizeof(unsigned long long), s));
+            PSK_TRY(induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_LMS_SUBSTRINGS, nullptr, n1, sa, s,
+                                   sorted));
+            uint32_t h[2];
+            PSK_TRY(ctx.read_u32((const uint32_t *)lmscnt, h, 2));
+            const unsigned long long got = ((unsigned long long)h[1] << 32) | h[0];
+            if (got != n1)
+                return set_error(PSACAK_EINTERNAL, "level %u: %llu LMS extracted by the S scan, expected %llu", level,
+                                 got, (unsigned long long)n1);
+            extracted = true;
+        } else {
             PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_LMS_SUBSTRINGS, nullptr, n1,
                                        cursor, sa, s));
+        }
     } else {
         PSK_TRY(induce_doubling<C>(ctx, text, n, types, lms, geom, nbuckets, INDUCE_LMS_SUBSTRINGS, nullptr, n1,
                                    cursor, sa, s));
@@ -199,10 +213,9 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     ctx.mark("induce lms-substrings", level);
 
     // Stage 2: name them and build the reduced string.
-    DBuf<uint32_t> sorted, red, heads, flags, sa1, names1;
+    DBuf<uint32_t> red, heads, flags, sa1, names1;
     uint32_t k = 0;
-    PSK_TRY(sorted.init(ctx, n1));
-    if (n1 > 0) {
+    if (n1 > 0 && !extracted) {
         PSK_TRY(ctx.compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_scalars + 1,
                             "extract_lms"));
         uint32_t got = 0;
@@ -210,6 +223,8 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         if (got != n1)
             return set_error(PSACAK_EINTERNAL, "level %u: %u LMS after the induced sort, expected %llu", level, got,
                              (unsigned long long)n1);
+    }
+    if (n1 > 0) {
         PSK_TRY(red.init(ctx, n1));
         PSK_TRY(heads.init(ctx, n1 + 1));
         PSK_TRY(flags.init(ctx, n1));
@@ -446,8 +461,8 @@ status_t ctx_init(Ctx &c, int device) {
     PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_err, sizeof(uint32_t)));
     PSK_CUDA(cudaMemset(c.d_err, 0, sizeof(uint32_t)));
-    PSK_CUDA(cudaMalloc(&c.d_induced, sizeof(unsigned long long)));
-    PSK_CUDA(cudaMemset(c.d_induced, 0, sizeof(unsigned long long)));
+    PSK_CUDA(cudaMalloc(&c.d_induced, 2 * sizeof(unsigned long long)));
+    PSK_CUDA(cudaMemset(c.d_induced, 0, 2 * sizeof(unsigned long long)));
     c.scan_ctas = 4 * (uint32_t)c.dev.num_sms;
     c.radix_ctas = 4 * (uint32_t)c.dev.num_sms;
     if (c.scan_ctas > MAX_CHUNKS) c.scan_ctas = MAX_CHUNKS;

@@ -70,8 +70,10 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
 // Bucket-ordered induced sort of a byte level (the reference's induce scan
 // processed one bucket at a time): every bucket's L part is completed and
 // then scattered to the higher buckets in scan order; the S scan mirrors it.
+// In INDUCE_LMS_SUBSTRINGS mode with `lms_out` set, the S scan also writes the
+// n1 LMS positions in sorted-substring order to lms_out.
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms,
                         const ByteGeom &hgeom, const ByteGeom *dgeom, InduceMode mode, const uint32_t *sorted_lms,
-                        uint64_t n1, uint32_t *sa, cudaStream_t s);
+                        uint64_t n1, uint32_t *sa, cudaStream_t s, uint32_t *lms_out = nullptr);
 
 }  // namespace psk

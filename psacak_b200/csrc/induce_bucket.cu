@@ -174,6 +174,15 @@ __global__ void k_place_cells(const uint32_t *__restrict__ vals, uint32_t ncells
 // scan) than the bucket's character c, and the predecessor goes to slot
 // cur_in[c0] + rank (L) or cur_in[c0] - 1 - rank (S) -- the reference's
 // bucket-pointer increment/decrement, in scan order.
+//
+// In the LMS-substring round the S scan also extracts the sorted LMS
+// substrings: an S-part entry whose predecessor is larger is an LMS
+// suffix (the reference keeps exactly these after its left_most clearing
+// and compacts them, src/psacak8.rs:35).  They get the spare digit 255
+// (never an S-scan target: targets are smaller than c) and go to the
+// bucket's range of the sorted LMS list, highest first.
+constexpr uint32_t LMS_DIGIT = 255;
+
 template <bool LSCAN> struct BucketPolicy {
     using Item = uint32_t;
     static constexpr int kMinBlocks = 4;
@@ -186,6 +195,9 @@ template <bool LSCAN> struct BucketPolicy {
     unsigned long long *induced;
     uint64_t n;
     uint32_t *err;
+    uint32_t *lms_out;   // S scan, LMS-substring round: sorted LMS list (else null)
+    uint32_t lms_hi;     // index of this bucket's last entry in that list
+    uint32_t lms_cap;    // entries of the list
     __device__ __forceinline__ void load(uint64_t i, Item &it, uint32_t &d) const {
         uint32_t x = sa[seq.slot((uint32_t)i)];
         d = 256;
@@ -194,17 +206,31 @@ template <bool LSCAN> struct BucketPolicy {
             if (LSCAN ? c0 > c : c0 < c) {
                 d = c0;
                 it = x - 1;
+            } else if (!LSCAN && lms_out && c0 > c && i < seq.a_len) {
+                d = LMS_DIGIT;
+                it = x;
             }
         }
     }
     __device__ __forceinline__ uint64_t out(uint32_t d, uint64_t r) const {
+        if (!LSCAN && lms_out && d == LMS_DIGIT) return (uint64_t)lms_hi - r;
         return LSCAN ? (uint64_t)cur_in[d] + r : (uint64_t)cur_in[d] - 1 - r;
     }
-    __device__ __forceinline__ void store(uint64_t idx, const Item &it) const {
+    __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t d) const {
+        if (!LSCAN && lms_out && d == LMS_DIGIT) {
+            if (idx < lms_cap) lms_out[idx] = it;
+            else dev_fail(err, DEVERR_RANGE);
+            return;
+        }
         if (idx < n) sa[idx] = it;
         else dev_fail(err, DEVERR_RANGE);
     }
     __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
+        if (!LSCAN && lms_out && d == LMS_DIGIT) {
+            cur_out[d] = cur_in[d];
+            if (total) atomicAdd(induced + 1, (unsigned long long)total);
+            return;
+        }
         cur_out[d] = LSCAN ? cur_in[d] + total : cur_in[d] - total;
         if (total) atomicAdd(induced, (unsigned long long)total);
     }
@@ -253,14 +279,15 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
 // cur[256..512) (the caller swaps the halves afterwards).
 template <bool LSCAN>
 static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t n, BucketSeq seq, uint8_t c,
-                           const uint32_t *cur_in, uint32_t *cur_out, cudaStream_t s) {
+                           const uint32_t *cur_in, uint32_t *cur_out, cudaStream_t s, uint32_t *lms_out = nullptr,
+                           uint32_t lms_hi = 0, uint32_t lms_cap = 0) {
     uint32_t nitems = seq.a_len + seq.b_len;
     if (nitems == 0) {
         PSK_CUDA(cudaMemcpyAsync(cur_out, cur_in, 256 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         return PSACAK_OK;
     }
     PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 12 * OS_BLOCK) + 1));
-    BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err};
+    BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err, lms_out, lms_hi, lms_cap};
     // algorithmic bytes: each entry read (4) and its predecessor's character
     // (1); inducing entries written once (4, added from the device count).
     return onesweep<BucketPolicy<LSCAN>, 12>(pol, nitems, ctx.os, ctx.d_err, s, "induce_scatter", 5ull * nitems);
@@ -268,7 +295,7 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
 
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms, const ByteGeom &hg,
                         const ByteGeom *dgeom, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
-                        uint32_t *sa, cudaStream_t s) {
+                        uint32_t *sa, cudaStream_t s, uint32_t *lms_out) {
     uint32_t maxpart = 1, maxbucket = 1;
     for (int c = 0; c < 256; c++) {
         uint32_t cnt = hg.tail[c] - hg.head[c];
@@ -331,7 +358,9 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
                                   s));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
-        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, s));
+        const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;
+        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, s, extract ? lms_out : nullptr,
+                                  hg.lmsstart[c] + hg.lmscount[c] - 1, (uint32_t)n1));
         std::swap(curS, alt);
     }
     return PSACAK_OK;

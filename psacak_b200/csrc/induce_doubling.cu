@@ -236,6 +236,9 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
                                         (Tri *)ctx.d_partial, d_tri, OpTri(), ctx.scan_ctas, s)));
         uint32_t tri[4];
         PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
+        if (ctx.stage_timing)
+            fprintf(stderr, "[psacak]   doubling %c-scan h=%llu: %u items, %d key bits -> %u unresolved in %llu groups\n",
+                    STYPE ? 'S' : 'L', (unsigned long long)h, cnt, KB + GB, tri[2], (unsigned long long)tri[3]);
         cnt = tri[2];
         ngroups = tri[3];
         std::swap(gA, gB);

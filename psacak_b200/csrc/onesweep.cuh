@@ -22,7 +22,7 @@
 //   out(digit, rank)                -> output index of the rank-th item of
 //                                      that digit (rank counts from 0 over all
 //                                      tiles of this launch)
-//   store(index, item)
+//   store(index, item, digit)
 //   finish(digit, total)            -> called once per digit by the last tile
 //   kMinBlocks                      -> CTAs per SM the register budget must allow
 #pragma once
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(OS_BLOCK, Policy::kMinBlocks) k_onesweep(Polic
     for (uint32_t i = threadIdx.x; i < tot; i += OS_BLOCK) {
         uint32_t dd = s_dig[i];
         uint64_t idx = pol.out(dd, (uint64_t)s_excl[dd] + (i - s_tstart[dd]));
-        pol.store(idx, s_item[i]);
+        pol.store(idx, s_item[i], dd);
     }
 }
 
@@ -206,7 +206,7 @@ template <class Pred, class Emit> struct CompactPolicy {
         }
     }
     __device__ __forceinline__ uint64_t out(uint32_t, uint64_t r) const { return r; }
-    __device__ __forceinline__ void store(uint64_t idx, const Item &it) const { emit((uint64_t)it, (uint32_t)idx); }
+    __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t) const { emit((uint64_t)it, (uint32_t)idx); }
     __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
         if (d == 0 && count) *count = total;
     }

@@ -34,7 +34,7 @@ template <class K, class V> struct RadixPolicy {
         d = (uint32_t)(it.k >> shift) & dmask;
     }
     __device__ __forceinline__ uint64_t out(uint32_t d, uint64_t r) const { return (uint64_t)base[d] + r; }
-    __device__ __forceinline__ void store(uint64_t idx, const Item &it) const {
+    __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t) const {
         kout[idx] = it.k;
         vout[idx] = it.v;
     }
