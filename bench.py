@@ -54,12 +54,32 @@ def parse():
     ap.add_argument("--cpu-window", type=int, default=16 << 20, help="bytes per CPU-oracle sample")
     ap.add_argument("--engine", type=int, default=0, help="psacak_schedule.engine (0 = auto)")
     ap.add_argument("--profile-json", default="", help="also write per-kernel stats here")
+    ap.add_argument("--workload", default="genome1g", choices=["genome1g", "batch4096", "zipf32", "iid8m"],
+                    help="genome1g (default, the headline), batch4096 (4096 texts in one batched build), "
+                         "zipf32 (psacak32 on 256M Zipf symbols), iid8m (8 MiB i.i.d. ACGT)")
+    ap.add_argument("--plain-texts", type=int, default=0,
+                    help="batch4096: time the per-text loop on this many texts (0 = all)")
     ap.add_argument("--single-build", action="store_true",
                     help="build the workload once and exit (for ncu launch lists)")
     return ap.parse_args()
 
 
 def workload_config(args):
+    if args.workload == "batch4096":
+        return {"workload": "batched psacak8: 4096 independent texts, lengths log-uniform 1 KiB..4 MiB, "
+                            "ACGT order-2 Markov (text i seeded by hash(seed, i)), one u32 SA per text",
+                "texts": 4096, "seed": args.seed, "engine": args.engine,
+                "l2_policy": "inputs larger than L2 (~2 GiB of texts, ~8 GiB of SAs); no flush",
+                "parallelism": "texts sharded across ranks (LPT)" if args.gpus > 1 else "single"}
+    if args.workload == "zipf32":
+        return {"workload": "psacak32 on 268435456 u32 symbols, alphabet 2^20, Zipf(1.1) frequencies, 10% planted "
+                            "repeats of length 1K..100K, u32 SA", "n": 1 << 28, "seed": args.seed,
+                "l2_policy": "inputs larger than L2 (1 GiB text + 1 GiB SA); no flush",
+                "parallelism": "replicas" if args.gpus > 1 else "single"}
+    if args.workload == "iid8m":
+        return {"workload": "psacak8 on 8 MiB i.i.d. uniform ACGT, u32 SA", "n": 8 << 20, "seed": args.seed,
+                "l2_policy": "8 MiB text + 32 MiB SA fit in L2; a 256 MiB buffer is written between steps",
+                "parallelism": "replicas" if args.gpus > 1 else "single"}
     return {
         "workload": "psacak8, genome-like u8 text of %d bytes (order-3 Markov ACGT, ~5%% N runs, ~30%% mutated "
                     "copies), u32 SA" % args.bytes,
@@ -215,6 +235,10 @@ def run_reference(args):
 
 # -- GPU arm -------------------------------------------------------------------
 def run_b200(args):
+    if args.workload == "batch4096":
+        return run_batch(args)
+    if args.workload == "zipf32":
+        return run_zipf32(args)
     import torch
     import psacak_b200 as pk
 
@@ -230,9 +254,15 @@ def run_b200(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    text = make_text(args)
+    if args.workload == "iid8m":
+        from psacak_b200 import synth
+        args.bytes = 8 << 20
+        text = synth.iid(args.bytes, b"ACGT", seed=args.seed)
+    else:
+        text = make_text(args)
     n = text.size
     ctx = pk.Context(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if args.workload == "iid8m" else None
     sched = {"engine": args.engine}
     d_text = torch.from_numpy(text).to(dev)
     d_sa = torch.empty(n, dtype=torch.int32, device=dev)
@@ -266,16 +296,29 @@ def run_b200(args):
     l0 = ctx.kernel_launches()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        build()
-    e1.record(stream)
+    if flush is None:
+        e0.record(stream)
+        for _ in range(args.steps):
+            build()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        step_ms_total = e0.elapsed_time(e1)
+    else:
+        # small input: flush L2 between steps, time only the builds
+        step_ms_total = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0.record(stream)
+            build()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            step_ms_total += e0.elapsed_time(e1)
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     launches = (ctx.kernel_launches() - l0) // max(args.steps, 1)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = step_ms_total / args.steps
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -350,6 +393,263 @@ def run_b200(args):
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
             "verified": verified, "levels": [[lv["m"], lv["n_lms"], lv["k"]] for lv in trace],
         }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _dist_init(torch, world, local):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def _max_over_ranks(torch, dist, dev, x):
+    if not dist:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _profile_roofline(ctx, build, torch, dev):
+    ctx.profile_reset()
+    ctx.profile(True)
+    build()
+    torch.cuda.synchronize(dev)
+    ctx.profile(False)
+    stats = ctx.profile_stats()
+    total_ms = sum(s["ms"] for s in stats)
+    dom = max((s for s in stats if s["bytes"] > 0), key=lambda s: s["ms"])
+    peak, peak_kind = measured_peak_hbm()
+    achieved = dom["bytes"] / (dom["ms"] / 1000.0) / 1e9
+    return {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": dominant_traffic(dom["name"], dom["items"] / max(dom["launches"], 1)),
+            "launches": dom["launches"], "algorithmic_bytes_per_launch": dom["bytes"] / max(dom["launches"], 1),
+            "avg_launch_ms": dom["ms"] / max(dom["launches"], 1),
+            "share_of_profiled_time": dom["ms"] / total_ms if total_ms else None}, stats
+
+
+def run_batch(args):
+    """Config 4: 4096 texts in one batched build, and the per-text loop beside it."""
+    import ctypes
+    import torch
+    import psacak_b200 as pk
+    from psacak_b200 import batch as pb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = _dist_init(torch, world, local)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    texts = pb.batch_texts(count=4096, seed=args.seed)
+    lens = [t.size for t in texts]
+    total_all = sum(lens)
+    mine = pb.shard_lpt(lens, world)[rank]
+    my_texts = [texts[i] for i in mine]
+    buf, off = pb.pack(my_texts)
+    n = int(buf.size)
+    ctx = pk.Context(local)
+    sched = {"engine": args.engine}
+    d_texts = torch.from_numpy(buf).to(dev)
+    d_sas = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def build():
+        ctx.psacak8_batch_dev(d_texts.data_ptr(), off, d_sas.data_ptr(), stream.cuda_stream, sched)
+
+    for _ in range(args.warmup):
+        build()
+    torch.cuda.synchronize(dev)
+    verified = None
+    if not args.no_verify:
+        verified = True
+        for i in range(len(my_texts)):
+            a, b = int(off[i]), int(off[i + 1])
+            if b > a and not ctx.check_sa8_dev(d_texts.data_ptr() + a, b - a, d_sas.data_ptr() + 4 * a,
+                                               stream.cuda_stream):
+                verified = False
+                break
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    l0 = ctx.kernel_launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        build()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = (ctx.kernel_launches() - l0) // max(args.steps, 1)
+    ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+    value = total_all / (ms / 1000.0)
+    roofline, stats = _profile_roofline(ctx, build, torch, dev)
+
+    # plain: the same texts, one psacak8_dev call each
+    k_plain = len(my_texts) if args.plain_texts <= 0 else min(args.plain_texts, len(my_texts))
+    torch.cuda.synchronize(dev)
+    p0 = time.perf_counter()
+    for i in range(k_plain):
+        a, b = int(off[i]), int(off[i + 1])
+        if b > a:
+            ctx.psacak8_dev(d_texts.data_ptr() + a, b - a, d_sas.data_ptr() + 4 * a, stream.cuda_stream, sched)
+    torch.cuda.synchronize(dev)
+    plain_s = time.perf_counter() - p0
+    plain_value = sum(int(off[i + 1] - off[i]) for i in range(k_plain)) / plain_s
+
+    e2e = None
+    if not args.no_e2e:
+        h_sas = [np.empty(t.size, dtype=np.uint32) for t in my_texts]
+        ptrs_t = (ctypes.c_void_p * len(my_texts))(*[t.ctypes.data for t in my_texts])
+        ptrs_s = (ctypes.c_void_p * len(my_texts))(*[x.ctypes.data for x in h_sas])
+        lens_c = (ctypes.c_uint64 * len(my_texts))(*[t.size for t in my_texts])
+        times = []
+        for i in range(args.e2e_steps + 1):
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            rc = pk.lib().psacak8_batch(ctx.handle, ptrs_t, lens_c, len(my_texts), ptrs_s, pk._sched_ptr(sched))
+            dt = time.perf_counter() - t0
+            if rc != 0:
+                pk._raise(rc)
+            if i > 0:
+                times.append(dt)
+        e2e_s = _max_over_ranks(torch, dist, dev, float(np.mean(times)))
+        e2e = {"value": total_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n, "d2h_bytes_per_step": 4 * n,
+               "ms_per_step": 1000.0 * e2e_s, "api": "psacak8_batch (host pointers, pageable per-text buffers)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        t0 = time.perf_counter()
+        done = 0
+        for t in my_texts:
+            oracle_lib.psacak8(t)
+            done += t.size
+            if time.perf_counter() - t0 > 5.0:
+                break
+        dt = time.perf_counter() - t0
+        cpu = {"value": done / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "oracle builds of the first %d bytes of the batch, text by text" % done}
+    if rank == 0:
+        line = {"metric": METRIC + " -- batched", "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                "config": workload_config(args), "e2e": e2e, "roofline": roofline,
+                "plain": {"value": plain_value, "unit": UNIT, "texts": k_plain,
+                          "api": "psacak8_dev per text, same device-resident texts"},
+                "batched_over_plain": value / plain_value, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": int(launches), "verified": verified, "total_bytes": total_all}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_zipf32(args):
+    """Config 3: psacak32 on 256M Zipf(1.1) symbols over 2^20 with planted repeats."""
+    import ctypes
+    import torch
+    import psacak_b200 as pk
+    from psacak_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = _dist_init(torch, world, local)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = 1 << 28
+    text = synth.zipf32(n, alphabet=1 << 20, s=1.1, repeat_frac=0.10, rep_min=1000, rep_max=100000, seed=args.seed)
+    ctx = pk.Context(local)
+    d_text = torch.from_numpy(text.view(np.int32)).to(dev)
+    d_sa = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def build():
+        ctx.psacak32_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        build()
+    torch.cuda.synchronize(dev)
+    verified = None if args.no_verify else ctx.check_sa32_dev(d_text.data_ptr(), n, d_sa.data_ptr(),
+                                                              stream.cuda_stream)
+    trace = ctx.trace()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    l0 = ctx.kernel_launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        build()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = (ctx.kernel_launches() - l0) // max(args.steps, 1)
+    ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+    value = world * n / (ms / 1000.0)
+    roofline, _ = _profile_roofline(ctx, build, torch, dev)
+    e2e = None
+    if not args.no_e2e:
+        h_text = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        h_text.numpy()[:] = text.view(np.int32)
+        h_sa = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        times = []
+        for i in range(args.e2e_steps + 1):
+            t0 = time.perf_counter()
+            rc = pk.lib().psacak32_ctx(ctx.handle, ctypes.c_void_p(h_text.data_ptr()), n,
+                                       ctypes.c_void_p(h_sa.data_ptr()), None)
+            dt = time.perf_counter() - t0
+            if rc != 0:
+                pk._raise(rc)
+            if i > 0:
+                times.append(dt)
+        e2e_s = _max_over_ranks(torch, dist, dev, float(np.mean(times)))
+        e2e = {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n,
+               "ms_per_step": 1000.0 * e2e_s, "api": "psacak32_ctx (host pointers, pinned buffers)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        w = 4 << 20
+        t0 = time.perf_counter()
+        oracle_lib.psacak32(text[:w].copy())
+        dt = time.perf_counter() - t0
+        cpu = {"value": w / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "first %d symbols of the workload, one serial oracle build" % w}
+    if rank == 0:
+        line = {"metric": "suffixes/sec (psacak32 suffix-array build, bit-exact)", "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic", "config": workload_config(args), "e2e": e2e, "roofline": roofline,
+                "hbm_gbs_algorithmic_build": algorithmic_build_bytes(trace, 12 * n) / (ms / 1000.0) / 1e9,
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches), "verified": verified,
+                "levels": [[lv["m"], lv["n_lms"], lv["k"]] for lv in trace]}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

@@ -42,11 +42,12 @@ extern "C" {
 /* Tunables of one build.  Zero fields mean "use the default".  Every
  * schedule gives the same suffix array; it only changes speed. */
 typedef struct {
-    uint32_t engine;          /* PSACAK_ENGINE_* for level 0 */
-    uint32_t inner_engine;    /* PSACAK_ENGINE_* for levels >= 1 */
-    uint32_t radix_ctas_per_sm; /* CTAs per SM of the radix/scan kernels */
-    uint32_t small_level;     /* levels shorter than this use the small-level path */
-    uint32_t reserved[4];
+    uint32_t engine;           /* PSACAK_ENGINE_* for level 0 */
+    uint32_t inner_engine;     /* PSACAK_ENGINE_* for levels >= 1 */
+    uint32_t scan_ctas_per_sm; /* CTAs per SM of the chunked scans (0 = 4) */
+    uint32_t batch_chunk_mib;  /* batch builds: max MiB per concatenated build (0 = 3072) */
+    uint32_t tile_items;       /* items per thread of the single-pass scatter: 8, 12 or 16 (0 = 12) */
+    uint32_t reserved[3];
 } psacak_schedule;
 
 /* One record per recursion level of the last build on a context. */
@@ -114,6 +115,17 @@ PSACAK_API int psacak32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n,
  */
 PSACAK_API int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *lens,
                   uint32_t n_texts, uint32_t *const *sas, const psacak_schedule *sched);
+
+/*
+ * psacak8_batch_dev -- device form of psacak8_batch: the texts are packed back
+ * to back in d_texts, text i occupying bytes [offsets[i], offsets[i+1]) (a
+ * host array of n_texts + 1 entries); text i's SA is written to
+ * d_sas[offsets[i] .. offsets[i+1]).  All texts are sorted by one build of
+ * their concatenation with a separator smaller than every byte, then split
+ * by text.
+ */
+PSACAK_API int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *offsets, uint32_t n_texts,
+                                 uint32_t *d_sas, void *stream, const psacak_schedule *sched);
 
 /* Per-level records of the last build on `ctx` (see psacak_level_info). */
 PSACAK_API int psacak_get_trace(psacak_ctx *ctx, psacak_level_info *out, uint32_t cap, uint32_t *count);

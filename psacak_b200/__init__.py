@@ -57,9 +57,10 @@ class Schedule(ctypes.Structure):
     _fields_ = [
         ("engine", ctypes.c_uint32),
         ("inner_engine", ctypes.c_uint32),
-        ("radix_ctas_per_sm", ctypes.c_uint32),
-        ("small_level", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("scan_ctas_per_sm", ctypes.c_uint32),
+        ("batch_chunk_mib", ctypes.c_uint32),
+        ("tile_items", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -114,6 +115,8 @@ def lib():
         L.psacak8_dev.argtypes = [p, p, u64, p, p, p]
         L.psacak32_dev.argtypes = [p, p, u64, p, p, p]
         L.psacak8_batch.argtypes = [p, p, p, u32, p, p]
+        L.psacak8_batch_dev.argtypes = [p, p, p, u32, p, p, p]
+        L.psacak8_batch_dev.restype = i32
         L.psacak_get_trace.argtypes = [p, p, u32, ctypes.POINTER(u32)]
         L.psacak_check_sa8_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
         L.psacak_check_sa32_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
@@ -218,6 +221,12 @@ class Context:
     def psacak32_dev(self, d_text, n, d_sa, stream=0, schedule=None):
         _raise(lib().psacak32_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
                                   ctypes.c_void_p(stream), _sched_ptr(schedule)))
+
+    def psacak8_batch_dev(self, d_texts, offsets, d_sas, stream=0, schedule=None):
+        """Texts packed in device memory; `offsets` (len = texts + 1) host ints."""
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        _raise(lib().psacak8_batch_dev(self._h, ctypes.c_void_p(d_texts), _vp(off), off.size - 1,
+                                       ctypes.c_void_p(d_sas), ctypes.c_void_p(stream), _sched_ptr(schedule)))
 
     def check_sa8_dev(self, d_text, n, d_sa, stream=0):
         ok = ctypes.c_int(0)

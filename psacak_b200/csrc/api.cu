@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <memory>
+#include <vector>
 
 #include "ctx.cuh"
 #include "induce.cuh"
@@ -303,6 +304,11 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     }
 }
 
+template status_t build_level<uint8_t>(Ctx &, const uint8_t *, const uint32_t *, const uint32_t *, uint64_t, uint64_t,
+                                       uint32_t *, uint32_t);
+
+status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, uint32_t ntexts, uint32_t *d_sas);
+
 // ---------------------------------------------------------------------------
 // translate_sample on the device (src/psacak32.rs:912-943): the distinct
 // symbols in order give buckets; an L-type symbol becomes its bucket head
@@ -493,8 +499,10 @@ static void apply_schedule(Ctx &c, const psacak_schedule *sched) {
     psacak_schedule d{};
     if (sched) d = *sched;
     c.sched = d;
-    uint32_t per = d.radix_ctas_per_sm ? d.radix_ctas_per_sm : 4;
-    c.radix_ctas = per * (uint32_t)c.dev.num_sms;
+    uint32_t per = d.scan_ctas_per_sm ? d.scan_ctas_per_sm : 4;
+    c.scan_ctas = per * (uint32_t)c.dev.num_sms;
+    if (c.scan_ctas > MAX_CHUNKS) c.scan_ctas = MAX_CHUNKS;
+    c.radix_ctas = 4 * (uint32_t)c.dev.num_sms;
     if (c.radix_ctas > RADIX_MAX_CTAS) c.radix_ctas = RADIX_MAX_CTAS;
 }
 
@@ -762,16 +770,73 @@ uint64_t psacak_kernel_launches(psacak_ctx *ctx) {
     return g_kernel_launches.load();
 }
 
+int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *offsets, uint32_t n_texts,
+                      uint32_t *d_sas, void *stream, const psacak_schedule *sched) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    if (n_texts > 0 && (!offsets || !d_texts || !d_sas)) return set_error(PSACAK_EINVAL, "null batch pointers");
+    for (uint32_t i = 0; i < n_texts; i++)
+        if (offsets[i + 1] < offsets[i]) return set_error(PSACAK_EINVAL, "batch offsets decrease at text %u", i);
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = stream ? (cudaStream_t)stream : c.own_stream;
+    apply_schedule(c, sched);
+    c.trace.clear();
+    PSK_TRY(c.arena_prepare());
+    ProfGuard pg(c);
+    status_t st = build_batch(c, d_texts, offsets, n_texts, d_sas);
+    if (st != PSACAK_OK) {
+        cudaStreamSynchronize(c.stream);
+        return st;
+    }
+    PSK_TRY(c.sync());
+    PSK_TRY(c.check_device_error());
+    PSK_TRY(profile_collect(c));
+    return PSACAK_OK;
+}
+
 int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *lens, uint32_t n_texts,
                   uint32_t *const *sas, const psacak_schedule *sched) {
     clear_error();
     if (!ctx) return set_error(PSACAK_EINVAL, "null context");
     if (n_texts > 0 && (!texts || !lens || !sas)) return set_error(PSACAK_EINVAL, "null batch arrays");
+    std::vector<uint64_t> off(n_texts + 1, 0);
     for (uint32_t i = 0; i < n_texts; i++) {
-        int rc = psacak8_ctx(ctx, texts[i], lens[i], sas[i], sched);
-        if (rc) return rc;
+        if (lens[i] > 0 && (!texts[i] || !sas[i])) return set_error(PSACAK_EINVAL, "null text or SA %u", i);
+        off[i + 1] = off[i] + lens[i];
     }
-    return PSACAK_OK;
+    if (off[n_texts] == 0) return PSACAK_OK;
+    Ctx &c = ctx->c;
+    status_t st;
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        PSK_CUDA(cudaSetDevice(c.dev.id));
+        c.stream = c.own_stream;
+        PSK_TRY(c.arena_prepare());
+    }
+    uint8_t *dt = nullptr;
+    uint32_t *ds = nullptr;
+    PSK_CUDA(cudaMallocAsync(&dt, off[n_texts], c.own_stream));
+    st = cudaMallocAsync(&ds, off[n_texts] * sizeof(uint32_t), c.own_stream) == cudaSuccess ? PSACAK_OK : PSACAK_ENOMEM;
+    if (st == PSACAK_OK) {
+        for (uint32_t i = 0; i < n_texts && st == PSACAK_OK; i++)
+            if (lens[i] && cudaMemcpyAsync(dt + off[i], texts[i], lens[i], cudaMemcpyHostToDevice, c.own_stream) !=
+                               cudaSuccess)
+                st = set_error(PSACAK_ECUDA, "batch upload of text %u failed", i);
+        if (st == PSACAK_OK) st = psacak8_batch_dev(ctx, dt, off.data(), n_texts, ds, c.own_stream, sched);
+        for (uint32_t i = 0; i < n_texts && st == PSACAK_OK; i++)
+            if (lens[i] && cudaMemcpyAsync(sas[i], ds + off[i], lens[i] * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                           c.own_stream) != cudaSuccess)
+                st = set_error(PSACAK_ECUDA, "batch download of SA %u failed", i);
+    } else {
+        set_error(PSACAK_ENOMEM, "batch: device allocation failed");
+    }
+    cudaStreamSynchronize(c.own_stream);
+    if (dt) cudaFreeAsync(dt, c.own_stream);
+    if (ds) cudaFreeAsync(ds, c.own_stream);
+    cudaStreamSynchronize(c.own_stream);
+    return st;
 }
 
 }  // extern "C"
