@@ -60,7 +60,8 @@ class Schedule(ctypes.Structure):
         ("scan_ctas_per_sm", ctypes.c_uint32),
         ("batch_chunk_mib", ctypes.c_uint32),
         ("tile_items", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("finish_below", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
 

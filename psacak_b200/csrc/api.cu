@@ -122,6 +122,13 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         return PSACAK_OK;
     }
     const bool bytes = sizeof(C) == 1;
+    if constexpr (sizeof(C) == 4) {
+        // recursion finisher: short inner strings are sorted by prefix doubling
+        if (names && bheads && ctx.sched.finish_below && n < ctx.sched.finish_below) {
+            trace_push(ctx, level, width, n, 0, 0, 0);
+            return sort_by_doubling(ctx, names, bheads, nbuckets, n, sa, s);
+        }
+    }
     const uint64_t nwords = ceil_div(n, 32);
     const uint64_t ntiles = ceil_div(n, TYPE_TILE);
     DBuf<uint32_t> types, lms, wcnt, pref, tscratch;

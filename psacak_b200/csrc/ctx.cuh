@@ -132,6 +132,11 @@ struct Ctx {
         if (stage_t0 > 0) fprintf(stderr, "[psacak] level %u %-24s %9.3f ms\n", level, what, t - stage_t0);
         stage_t0 = t;
     }
+    // Items per thread of the single-pass scatter (schedule tile_items).
+    int tile_ipt() const {
+        uint32_t t = sched.tile_items;
+        return (t == 8 || t == 16) ? (int)t : 12;
+    }
     // Grows the onesweep status array to hold `tiles` tiles.
     status_t ensure_onesweep(uint64_t tiles) {
         if (tiles <= os.max_tiles) return PSACAK_OK;
@@ -149,14 +154,14 @@ struct Ctx {
     // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).
     template <class K, class V>
     status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1) {
-        PSK_TRY(ensure_onesweep(ceil_div(n, 12 * OS_BLOCK) + 1));
-        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream);
+        PSK_TRY(ensure_onesweep(ceil_div(n, 8 * OS_BLOCK) + 1));
+        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream, tile_ipt());
     }
     // Single-pass stable compaction (see compact1).
     template <class Pred, class Emit>
     status_t compact(Pred pred, Emit emit, uint64_t n, uint32_t *count_out, const char *name) {
-        PSK_TRY(ensure_onesweep(ceil_div(n, 12 * OS_BLOCK) + 1));
-        return compact1(pred, emit, n, count_out, os, d_err, stream, name);
+        PSK_TRY(ensure_onesweep(ceil_div(n, 8 * OS_BLOCK) + 1));
+        return compact1(pred, emit, n, count_out, os, d_err, stream, name, tile_ipt());
     }
     status_t sync() {
         PSK_CUDA(cudaStreamSynchronize(stream));

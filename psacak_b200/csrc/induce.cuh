@@ -67,6 +67,10 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
                          Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
                          uint32_t *cursor, uint32_t *sa, cudaStream_t s);
 
+// Suffix array of a u32 level directly by prefix doubling (recursion finisher).
+status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bheads, uint64_t nbuckets, uint64_t n,
+                          uint32_t *sa, cudaStream_t s);
+
 // Bucket-ordered induced sort of a byte level (the reference's induce scan
 // processed one bucket at a time): every bucket's L part is completed and
 // then scattered to the higher buckets in scan order; the S scan mirrors it.

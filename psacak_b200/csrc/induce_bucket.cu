@@ -286,11 +286,12 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
         PSK_CUDA(cudaMemcpyAsync(cur_out, cur_in, 256 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         return PSACAK_OK;
     }
-    PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 12 * OS_BLOCK) + 1));
+    PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 8 * OS_BLOCK) + 1));
     BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err, lms_out, lms_hi, lms_cap};
     // algorithmic bytes: each entry read (4) and its predecessor's character
     // (1); inducing entries written once (4, added from the device count).
-    return onesweep<BucketPolicy<LSCAN>, 12>(pol, nitems, ctx.os, ctx.d_err, s, "induce_scatter", 5ull * nitems);
+    return onesweep_ipt<BucketPolicy<LSCAN>>(pol, nitems, ctx.tile_ipt(), ctx.os, ctx.d_err, s, "induce_scatter",
+                                              5ull * nitems);
 }
 
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms, const ByteGeom &hg,

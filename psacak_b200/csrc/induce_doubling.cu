@@ -124,6 +124,26 @@ template <class C, bool STYPE> struct WEmit {
     }
 };
 
+// Recursion finisher: every position is an item, grouped by its symbol's
+// bucket (head from the bucket boundaries), terminated only by the sentinel.
+struct AllPred {
+    __device__ __forceinline__ bool operator()(uint64_t) const { return true; }
+};
+struct AllEmit {
+    const uint32_t *names, *bheads;
+    uint32_t *Wg, *Wv, *R;
+    __device__ __forceinline__ void operator()(uint64_t j, uint32_t slot) const {
+        uint32_t id = names[j];
+        Wg[slot] = id;
+        Wv[slot] = (uint32_t)j;
+        R[j] = bheads[id] + 1;
+    }
+};
+__global__ void k_copy_heads(const uint32_t *bheads, uint64_t nbuckets, uint32_t *gstart) {
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nbuckets; c += (uint64_t)gridDim.x * blockDim.x)
+        gstart[c] = bheads[c];
+}
+
 template <class C, bool STYPE>
 __global__ void k_group_starts(Geom<C> g, uint64_t nbuckets, uint32_t *gstart) {
     for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nbuckets; c += (uint64_t)gridDim.x * blockDim.x)
@@ -201,6 +221,10 @@ struct RoundStore {
     }
 };
 
+static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, uint32_t *R, uint32_t *sa,
+                                uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1,
+                                uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s);
+
 // One scan (L or S): resolves the chains of every item of the given type.
 template <class C, bool STYPE>
 static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, Geom<C> geom,
@@ -216,6 +240,14 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
     PSK_TRY(ctx.compact(WPred<C, STYPE>{types}, WEmit<C, STYPE>{text, geom, Wg, Wv, R}, n, d_cnt, "double_items"));
     uint32_t cnt = 0;
     PSK_TRY(ctx.read_u32(d_cnt, &cnt));
+    return doubling_rounds(ctx, n, nbuckets, cnt, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, STYPE ? 'S' : 'L', s);
+}
+
+// Rank-doubling rounds over the work list (Wg = dense group id, Wv =
+// position) until every item has its own slot.
+static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, uint32_t *R, uint32_t *sa,
+                                uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1,
+                                uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s) {
     const int KB = bitlen(n);
     uint64_t ngroups = nbuckets;
     Tri *d_tri = (Tri *)(ctx.d_scalars + 4);
@@ -238,7 +270,7 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
         PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
         if (ctx.stage_timing)
             fprintf(stderr, "[psacak]   doubling %c-scan h=%llu: %u items, %d key bits -> %u unresolved in %llu groups\n",
-                    STYPE ? 'S' : 'L', (unsigned long long)h, cnt, KB + GB, tri[2], (unsigned long long)tri[3]);
+                    tag, (unsigned long long)h, cnt, KB + GB, tri[2], (unsigned long long)tri[3]);
         cnt = tri[2];
         ngroups = tri[3];
         std::swap(gA, gB);
@@ -280,6 +312,33 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
     PSK_TRY((doubling_scan<C, false>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));
     PSK_TRY((doubling_scan<C, true>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));
     return PSACAK_OK;
+}
+
+// Suffix array of a u32 string directly by prefix doubling (no recursion):
+// the items are all positions, grouped by bucket, ranks doubled until every
+// suffix is alone.  Rounds = log2 of the longest repeat, so this only pays
+// for short strings, where it replaces the remaining recursion levels.
+status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bheads, uint64_t nbuckets, uint64_t n,
+                          uint32_t *sa, cudaStream_t s) {
+    DBuf<uint32_t> R, Wg, Wv, v0, v1, gA, gB;
+    DBuf<uint64_t> k0, k1;
+    const uint64_t gcap = n > nbuckets ? n : nbuckets;
+    PSK_TRY(gA.init(ctx, gcap));
+    PSK_TRY(gB.init(ctx, gcap));
+    PSK_TRY(R.init(ctx, n + 1));
+    PSK_TRY(Wg.init(ctx, n));
+    PSK_TRY(Wv.init(ctx, n));
+    PSK_TRY(v0.init(ctx, n));
+    PSK_TRY(v1.init(ctx, n));
+    PSK_TRY(k0.init(ctx, n));
+    PSK_TRY(k1.init(ctx, n));
+    PSK_CUDA(cudaMemsetAsync(R.get() + n, 0, sizeof(uint32_t), s));
+    uint64_t gb = ceil_div(nbuckets, 256);
+    k_copy_heads<<<(uint32_t)(gb < 4096 ? gb : 4096), 256, 0, s>>>(bheads, nbuckets, gA);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    PSK_TRY(ctx.compact(AllPred{}, AllEmit{names, bheads, Wg, Wv, R}, n, ctx.d_scalars, "double_items"));
+    return doubling_rounds(ctx, n, nbuckets, (uint32_t)n, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, 'A', s);
 }
 
 template status_t induce_doubling<uint8_t>(Ctx &, const uint8_t *, uint64_t, const uint32_t *, const uint32_t *,

@@ -192,6 +192,15 @@ status_t onesweep(Policy pol, uint64_t n, OnesweepScratch &sc, uint32_t *err, cu
 
 namespace psk {
 
+// Runtime choice of the tile (items per thread: 8, 12 or 16).
+template <class Policy>
+status_t onesweep_ipt(Policy pol, uint64_t n, int ipt, OnesweepScratch &sc, uint32_t *err, cudaStream_t s,
+                      const char *pname, uint64_t pbytes) {
+    if (ipt == 8) return onesweep<Policy, 8>(pol, n, sc, err, s, pname, pbytes);
+    if (ipt == 16) return onesweep<Policy, 16>(pol, n, sc, err, s, pname, pbytes);
+    return onesweep<Policy, 12>(pol, n, sc, err, s, pname, pbytes);
+}
+
 // Stable compaction through the same kernel: kept items carry digit 0.
 template <class Pred, class Emit> struct CompactPolicy {
     using Item = uint32_t;
@@ -216,13 +225,12 @@ template <class Pred, class Emit> struct CompactPolicy {
 // slots consecutive in index order; *count_out (device, nullable) = kept.
 template <class Pred, class Emit>
 status_t compact1(Pred pred, Emit emit, uint64_t n, uint32_t *count_out, OnesweepScratch &sc, uint32_t *err,
-                  cudaStream_t s, const char *pname) {
+                  cudaStream_t s, const char *pname, int ipt = 12) {
     if (n == 0) {
         if (count_out) PSK_CUDA(cudaMemsetAsync(count_out, 0, sizeof(uint32_t), s));
         return PSACAK_OK;
     }
-    return onesweep<CompactPolicy<Pred, Emit>, 12>(CompactPolicy<Pred, Emit>{pred, emit, count_out}, n, sc, err, s,
-                                                   pname, 0);
+    return onesweep_ipt(CompactPolicy<Pred, Emit>{pred, emit, count_out}, n, ipt, sc, err, s, pname, 0);
 }
 
 }  // namespace psk

@@ -77,7 +77,8 @@ __global__ void k_radix_bases(const uint32_t *hist, uint32_t *bases);
 
 template <class K, class V>
 status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit, int end_bit, uint32_t *d_hist,
-                          uint32_t *h_hist, OnesweepScratch &sc, uint32_t *err, int *result_in_1, cudaStream_t s) {
+                          uint32_t *h_hist, OnesweepScratch &sc, uint32_t *err, int *result_in_1, cudaStream_t s,
+                          int ipt = 12) {
     *result_in_1 = 0;
     if (n <= 1 || end_bit <= begin_bit) return PSACAK_OK;
     const int npasses = (end_bit - begin_bit + 7) / 8;
@@ -102,8 +103,8 @@ status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit,
         int shift = begin_bit + 8 * p;
         int bits = end_bit - shift < 8 ? end_bit - shift : 8;
         RadixPolicy<K, V> pol{ki, vi, ko, vo, shift, (1u << bits) - 1, bases + p * 256};
-        constexpr int IPT = 12;
-        PSK_TRY((onesweep<RadixPolicy<K, V>, IPT>(pol, n, sc, err, s, "radix_pass", 2 * n * (sizeof(K) + sizeof(V)))));
+        PSK_TRY((onesweep_ipt<RadixPolicy<K, V>>(pol, n, ipt, sc, err, s, "radix_pass",
+                                                 2 * n * (sizeof(K) + sizeof(V)))));
         K *tk = ki; ki = ko; ko = tk;
         V *tv = vi; vi = vo; vo = tv;
         flip ^= 1;

@@ -106,3 +106,21 @@ def test_zipf32_4m(ctx):
     t = synth.zipf32(4 << 20, seed=3)
     sa = ctx.psacak32(t)
     assert (sa == o.psacak32(t)).all()
+
+
+SCHEDULES = [dict(engine=e, inner_engine=pk.ENGINE_DOUBLING, tile_items=t, finish_below=f)
+             for e in (pk.ENGINE_BUCKET, pk.ENGINE_DOUBLING) for t in (8, 12, 16) for f in (0, 1 << 14)]
+
+
+def test_every_schedule_gives_the_same_sa(ctx):
+    rng = np.random.default_rng(23)
+    texts = [synth.genome(300_000, seed=5), rng.integers(0, 3, 50_000).astype(np.uint8),
+             np.frombuffer(b"abracadabra" * 3000, np.uint8)]
+    for t in texts:
+        want = o.psacak8(t)
+        for sc in SCHEDULES:
+            assert (ctx.psacak(t, sc) == want).all(), sc
+    sym = synth.zipf32(200_000, alphabet=1 << 16, seed=6)
+    want = o.psacak32(sym)
+    for sc in SCHEDULES:
+        assert (ctx.psacak32(sym, sc) == want).all(), sc
