@@ -54,9 +54,12 @@ def parse():
     ap.add_argument("--cpu-window", type=int, default=16 << 20, help="bytes per CPU-oracle sample")
     ap.add_argument("--engine", type=int, default=0, help="psacak_schedule.engine (0 = auto)")
     ap.add_argument("--profile-json", default="", help="also write per-kernel stats here")
-    ap.add_argument("--workload", default="genome1g", choices=["genome1g", "batch4096", "zipf32", "iid8m"],
+    ap.add_argument("--workload", default="genome1g", choices=["genome1g", "batch4096", "zipf32", "iid8m", "serve"],
                     help="genome1g (default, the headline), batch4096 (4096 texts in one batched build), "
                          "zipf32 (psacak32 on 256M Zipf symbols), iid8m (8 MiB i.i.d. ACGT)")
+    ap.add_argument("--requests", type=int, default=20000, help="serve: number of requests")
+    ap.add_argument("--load", type=float, default=0.7, help="serve: arrival rate / measured capacity")
+    ap.add_argument("--regret-sample", type=int, default=200, help="serve: requests judged by exhaustive autotune")
     ap.add_argument("--plain-texts", type=int, default=0,
                     help="batch4096: time the per-text loop on this many texts (0 = all)")
     ap.add_argument("--single-build", action="store_true",
@@ -234,7 +237,36 @@ def run_reference(args):
 
 
 # -- GPU arm -------------------------------------------------------------------
+def run_serve(args):
+    """Config 5: Poisson stream of build requests with the learned selector."""
+    import torch
+    import psacak_b200 as pk
+    from psacak_b200 import selector as sel
+    from psacak_b200 import serve
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ctx = pk.Context(0)
+    model = os.path.join(ROOT, "psacak_b200", "models", "selector.npz")
+    net = sel.Selector.load(ctx, model) if os.path.exists(model) else None
+    res = serve.run(ctx, net, count=args.requests, seed=args.seed, load=args.load,
+                    autotune_sample=args.regret_sample, log=lambda m: print(m, file=sys.stderr, flush=True))
+    line = {"metric": "serving throughput (suffixes/s) with p50/p99 latency, learned schedule selector",
+            "value": res["throughput_suffixes_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32", "data": "synthetic",
+            "config": {"workload": "%d requests, Poisson arrivals at %.0f%% of measured capacity, lengths log-uniform "
+                                   "4 KiB..64 MiB symbols, half u8 ACGT / half u32 over 2^16 (device-generated "
+                                   "i.i.d.)" % (args.requests, 100 * args.load), "seed": args.seed,
+                       "selector": "trained model" if net is not None else "none (default schedule)"},
+            "serving": res}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_b200(args):
+    if args.workload == "serve":
+        return run_serve(args)
     if args.workload == "batch4096":
         return run_batch(args)
     if args.workload == "zipf32":

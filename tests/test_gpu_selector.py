@@ -1,0 +1,114 @@
+"""The schedule selector on the GPU: forward and backward kernels against the
+CPU fp32 reference (tolerance rtol 1e-3 / atol 1e-5), training, inference,
+statistics, and the gain of the trained network over the fixed default
+schedule on held-out texts (every schedule gives the same SA)."""
+import numpy as np
+import pytest
+
+import oracle_lib as o
+import psacak_b200 as pk
+from psacak_b200 import selector as sel, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = pk.Context(0)
+    yield c
+    c.close()
+
+
+def test_forward_and_gradients_match_reference(ctx):
+    rng = np.random.default_rng(1)
+    k = len(sel.SCHEDULES)
+    net = sel.Selector(ctx, k=k, seed=3)
+    p = net.params.cpu().numpy()
+    X = rng.standard_normal((53, sel.NF)).astype(np.float32)
+    T = rng.standard_normal((53, k)).astype(np.float32)
+    M = (rng.random((53, k)) > 0.25).astype(np.float32)
+    _, Y, _, _ = net.forward(X)
+    Yr, _, _, _ = sel.ref_forward(p, X, k)
+    np.testing.assert_allclose(Y.cpu().numpy(), Yr, rtol=1e-3, atol=1e-5)
+    loss, G = net.gradients(X, T, M)
+    lr_, gr = sel.ref_gradients(p, X, T, M, k)
+    assert abs(loss - lr_) <= 1e-3 * max(1.0, abs(lr_))
+    np.testing.assert_allclose(G.cpu().numpy(), gr, rtol=1e-3, atol=1e-5)
+
+
+def test_training_fits_and_inference_is_argmin(ctx):
+    rng = np.random.default_rng(2)
+    k = 6
+    X = rng.standard_normal((200, sel.NF)).astype(np.float32)
+    X[:, -1] = 1.0
+    W = rng.standard_normal((sel.NF, k)).astype(np.float32) * 0.5
+    T = (np.tanh(X @ W) * 2.0).astype(np.float32)
+    net = sel.Selector(ctx, k=k, seed=4)
+    hist = net.train(X, T, np.ones_like(T), epochs=600, lr=3e-3)
+    assert hist[-1] < 0.25 * hist[0]
+    _, Y, _, _ = net.forward(X[:20])
+    Y = Y.cpu().numpy()
+    for i in range(20):
+        c, pred = net.predict(X[i])
+        np.testing.assert_allclose(pred, Y[i], rtol=1e-4, atol=1e-5)
+        assert c == int(np.argmin(pred))
+
+
+def test_text_statistics(ctx):
+    t = synth.iid(1 << 20, b"ACGT", seed=7)
+    d = torch.from_numpy(t).cuda()
+    f = sel.features(ctx, d.data_ptr(), t.size, 1)
+    assert f.shape == (16,) and f[-1] == 1.0
+    assert abs(f[0] - np.log2(t.size + 1) / 32) < 1e-5 and f[1] == 0.25
+    assert 0.2 < f[3] < 0.45          # LMS density of i.i.d. ACGT (~1/3)
+    assert 0.15 < f[5] < 0.35         # equal neighbours (~1/4)
+    rep = np.tile(synth.iid(4096, b"ACGT", seed=8), 64)
+    fr = sel.features(ctx, torch.from_numpy(rep).cuda().data_ptr(), rep.size, 1)
+    assert fr[6] > f[6]               # repeats are seen
+
+
+def test_selector_gains_over_default_schedule(ctx):
+    """Train on autotuned timings of training texts, then compare the picks
+    with the fixed default schedule on held-out texts."""
+    rng = np.random.default_rng(5)
+
+    def texts(count, seed):
+        out = []
+        for i in range(count):
+            n = int(np.exp(rng.uniform(np.log(8 << 10), np.log(2 << 20))))
+            if i % 2 == 0:
+                out.append((synth.genome(n, seed=seed + i), 1))
+            else:
+                out.append((synth.zipf32(n // 4 + 16, alphabet=1 << 16, repeat_frac=0.0, seed=seed + i), 4))
+        return out
+
+    def measure(items):
+        X, Tm = [], []
+        for t, w in items:
+            d = torch.from_numpy(t.view(np.int32) if w == 4 else t).cuda()
+            sa = torch.empty(t.size, dtype=torch.int32, device="cuda")
+            X.append(sel.features(ctx, d.data_ptr(), t.size, w))
+            Tm.append(sel.autotune(ctx, d.data_ptr(), t.size, w, sa.data_ptr(), reps=2))
+        return np.array(X), np.array(Tm)
+
+    Xtr, Ttr = measure(texts(24, 100))
+    Xte, Tte = measure(texts(10, 900))
+    T, M = sel.targets(Ttr)
+    net = sel.Selector(ctx, seed=6)
+    net.train(Xtr, T, M, epochs=1500, lr=3e-3)
+    picks = [net.predict(x)[0] for x in Xte]
+    sel_ms = sum(Tte[i, p] for i, p in enumerate(picks))
+    def_ms = Tte[:, sel.DEFAULT_INDEX].sum()
+    best_ms = Tte.min(axis=1).sum()
+    print("held-out: best %.2f ms, selector %.2f ms, default %.2f ms" % (best_ms, sel_ms, def_ms))
+    assert sel_ms <= def_ms * 1.02
+    # a picked schedule still builds the oracle's suffix array
+    t, w = texts(1, 7000)[0]
+    d = torch.from_numpy(t.view(np.int32) if w == 4 else t).cuda()
+    sa = torch.empty(t.size, dtype=torch.int32, device="cuda")
+    c, _ = net.predict(sel.features(ctx, d.data_ptr(), t.size, w))
+    sel.build(ctx, d.data_ptr(), t.size, w, sa.data_ptr(), 0, sel.SCHEDULES[c])
+    torch.cuda.synchronize()
+    want = o.psacak8(t) if w == 1 else o.psacak32(t)
+    assert (sa.cpu().numpy().view(np.uint32) == want).all()
