@@ -522,7 +522,8 @@ struct ProfGuard {
 };
 
 // Folds the device-side count of entries scattered by the bucket scans into
-// the "induce_scatter" class (4 bytes read + 4 bytes written per entry).
+// the "induce_scatter" class (per entry: the entry and its predecessor
+// character written, 5 bytes, and one text byte read in front of it).
 static status_t profile_collect(Ctx &c) {
     if (!c.profiling) return PSACAK_OK;
     c.prof.resolve();
@@ -532,7 +533,7 @@ static status_t profile_collect(Ctx &c) {
     unsigned long long induced = ((unsigned long long)h[1] << 32) | h[0];
     if (induced) {
         int cls = c.prof.cls_of("induce_scatter");
-        c.prof.stats[cls].bytes += 8ull * induced;
+        c.prof.stats[cls].bytes += 6ull * induced;
     }
     return PSACAK_OK;
 }

@@ -60,7 +60,7 @@ constexpr int PL_BLOCK = 256;
 __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__restrict__ text, uint64_t nwords,
                                                              const uint32_t *__restrict__ lms,
                                                              const ByteGeom *__restrict__ g, uint32_t *cursor,
-                                                             uint32_t *sa, uint64_t wchunk) {
+                                                             uint32_t *sa, uint8_t *c0s, uint64_t wchunk) {
     __shared__ uint32_t s_cnt[256], s_base[256];
     s_cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -79,8 +79,10 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
             if (on && (int)lane == leader) got = atomicAdd(&s_cnt[c], __popc(peers));
             got = __shfl_sync(FULL_MASK, got, leader);
             if (pass == 1 && on) {
-                uint32_t slot = s_base[c] + got + __popc(peers & lt);
-                sa[g->tail[c] - 1 - slot] = (uint32_t)((w << 5) + lane);
+                const uint32_t slot = g->tail[c] - 1 - (s_base[c] + got + __popc(peers & lt));
+                const uint64_t p = (w << 5) + lane;  // LMS positions are > 0
+                sa[slot] = (uint32_t)p;
+                c0s[slot] = text[p - 1];
             }
         }
         __syncthreads();
@@ -94,36 +96,55 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
 }
 
 __global__ void k_place_lms_sorted8(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sorted,
-                                    uint64_t n1, const ByteGeom *__restrict__ g, uint32_t *sa) {
+                                    uint64_t n1, const ByteGeom *__restrict__ g, uint32_t *sa, uint8_t *c0s) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t p = sorted[i];
         uint8_t c = text[p];
-        sa[g->tail[c] - g->lmscount[c] + ((uint32_t)i - g->lmsstart[c])] = p;
+        uint32_t slot = g->tail[c] - g->lmscount[c] + ((uint32_t)i - g->lmsstart[c]);
+        sa[slot] = p;
+        c0s[slot] = text[p - 1];
     }
 }
 
 // cursors: L scan starts at the bucket heads, S scan at the tails; the
 // sentinel suffix n-1 is the first entry of its bucket (src/psacak8.rs:131-135).
 __global__ void k_init_cursors(const ByteGeom *__restrict__ g, const uint8_t *__restrict__ text, uint64_t n,
-                               uint32_t *curL, uint32_t *curS, uint32_t *sa) {
+                               uint32_t *curL, uint32_t *curS, uint32_t *sa, uint8_t *c0s) {
     int c = threadIdx.x;
     uint8_t last = text[n - 1];
     curL[c] = g->head[c] + (c == last ? 1u : 0u);
     curS[c] = g->tail[c];
-    if (c == 0) sa[g->head[last]] = (uint32_t)(n - 1);
+    if (c == 0) {
+        sa[g->head[last]] = (uint32_t)(n - 1);
+        c0s[g->head[last]] = n >= 2 ? text[n - 2] : 0;
+    }
 }
 
 // ---- chain expansion -----------------------------------------------------
 
 // Seeds in scan order: L part = sa[start + q]; S part = sa[start - q].
-// runs[q] = number of equal characters c in front of the seed.
+// runs[q] = number of equal characters c in front of the seed; endc[q] =
+// the character in front of the run.  c0s[slot] (the character in front of
+// sa[slot]) was written beside every seed by whoever placed it, so the text
+// is only read inside runs.
 __global__ void k_seed_runs(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sa, uint32_t start, int dir,
-                            uint32_t nseeds, uint8_t c, uint32_t *runs, uint32_t *maxrun) {
+                            uint32_t nseeds, uint8_t c, uint32_t *runs, uint32_t *maxrun, const uint8_t *c0s,
+                            uint8_t *endc) {
     uint32_t mx = 0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nseeds; q += gridDim.x * blockDim.x) {
-        uint32_t x = sa[dir > 0 ? start + q : start - q];
+        const uint32_t slot = dir > 0 ? start + q : start - q;
+        uint32_t x = sa[slot];
         uint32_t r = 0;
-        while (r < x && text[x - r - 1] == c) r++;
+        uint8_t before = 0;
+        if (x > 0) {
+            before = c0s[slot];
+            if (before == c) {
+                r = 1;
+                while (r < x && (before = text[x - r - 1]) == c) r++;
+                if (r == x) before = 0;
+            }
+        }
+        endc[q] = before;
         runs[q] = r;
         mx = r > mx ? r : mx;
     }
@@ -143,9 +164,13 @@ struct RunStore {
     __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t) const { off[i] = excl; }
 };
 
-// Cell q (row-major over seeds) -> (depth d, value seed - d).
+// Cell q (row-major over seeds) -> (depth d, value (seed - d) << 8 | the
+// character in front of that suffix: c inside the run, the run's leading
+// character at its deepest member).
 __global__ void k_expand_cells(const uint32_t *__restrict__ sa, uint32_t start, int dir, uint32_t nseeds,
-                               const uint32_t *__restrict__ off, uint32_t ncells, uint32_t *keys, uint32_t *vals) {
+                               const uint32_t *__restrict__ off, const uint32_t *__restrict__ runs,
+                               const uint8_t *__restrict__ endc, uint8_t c, uint32_t ncells, uint32_t *keys,
+                               uint64_t *vals) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ncells; q += gridDim.x * blockDim.x) {
         // last seed s with off[s] <= q
         uint32_t lo = 0, hi = nseeds - 1;
@@ -156,15 +181,20 @@ __global__ void k_expand_cells(const uint32_t *__restrict__ sa, uint32_t start, 
         }
         uint32_t d = q - off[lo] + 1;
         uint32_t x = sa[dir > 0 ? start + lo : start - lo];
+        uint8_t pc = d < runs[lo] ? c : endc[lo];
         keys[q] = d;
-        vals[q] = x - d;
+        vals[q] = ((uint64_t)(x - d) << 8) | pc;
     }
 }
 
-__global__ void k_place_cells(const uint32_t *__restrict__ vals, uint32_t ncells, uint32_t first, int dir,
-                              uint32_t *sa) {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ncells; q += gridDim.x * blockDim.x)
-        sa[dir > 0 ? first + q : first - q] = vals[q];
+__global__ void k_place_cells(const uint64_t *__restrict__ vals, uint32_t ncells, uint32_t first, int dir,
+                              uint32_t *sa, uint8_t *c0s) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ncells; q += gridDim.x * blockDim.x) {
+        uint32_t slot = dir > 0 ? first + q : first - q;
+        uint64_t v = vals[q];
+        sa[slot] = (uint32_t)(v >> 8);
+        c0s[slot] = (uint8_t)v;
+    }
 }
 
 // ---- multisplit ----------------------------------------------------------
@@ -183,9 +213,13 @@ __global__ void k_place_cells(const uint32_t *__restrict__ vals, uint32_t ncells
 // bucket's range of the sorted LMS list, highest first.
 constexpr uint32_t LMS_DIGIT = 255;
 
+// Items carry the target position (low 32 bits) and the character in front
+// of it (bits 32..39), stored beside the entry in c0s, so that every entry's
+// predecessor character is gathered from the text once, in the same sector
+// read that finds the entry's own predecessor.
 template <bool LSCAN> struct BucketPolicy {
-    using Item = uint32_t;
-    static constexpr int kMinBlocks = 4;
+    using Item = uint64_t;
+    static constexpr int kMinBlocks = 3;
     const uint8_t *text;
     uint32_t *sa;
     BucketSeq seq;
@@ -198,14 +232,16 @@ template <bool LSCAN> struct BucketPolicy {
     uint32_t *lms_out;   // S scan, LMS-substring round: sorted LMS list (else null)
     uint32_t lms_hi;     // index of this bucket's last entry in that list
     uint32_t lms_cap;    // entries of the list
+    uint8_t *c0s;        // c0s[slot] = text[sa[slot] - 1] for every placed entry
     __device__ __forceinline__ void load(uint64_t i, Item &it, uint32_t &d) const {
-        uint32_t x = sa[seq.slot((uint32_t)i)];
+        const uint32_t slot = seq.slot((uint32_t)i);
+        uint32_t x = sa[slot];
         d = 256;
         if (x > 0) {
-            uint32_t c0 = text[x - 1];
+            uint32_t c0 = c0s[slot];
             if (LSCAN ? c0 > c : c0 < c) {
                 d = c0;
-                it = x - 1;
+                it = (uint64_t)(x - 1) | ((uint64_t)(x >= 2 ? text[x - 2] : 0) << 32);
             } else if (!LSCAN && lms_out && c0 > c && i < seq.a_len) {
                 d = LMS_DIGIT;
                 it = x;
@@ -218,12 +254,16 @@ template <bool LSCAN> struct BucketPolicy {
     }
     __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t d) const {
         if (!LSCAN && lms_out && d == LMS_DIGIT) {
-            if (idx < lms_cap) lms_out[idx] = it;
+            if (idx < lms_cap) lms_out[idx] = (uint32_t)it;
             else dev_fail(err, DEVERR_RANGE);
             return;
         }
-        if (idx < n) sa[idx] = it;
-        else dev_fail(err, DEVERR_RANGE);
+        if (idx < n) {
+            sa[idx] = (uint32_t)it;
+            c0s[idx] = (uint8_t)(it >> 32);
+        } else {
+            dev_fail(err, DEVERR_RANGE);
+        }
     }
     __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
         if (!LSCAN && lms_out && d == LMS_DIGIT) {
@@ -245,17 +285,18 @@ static inline uint32_t grid_cap(uint64_t n, uint32_t cap) {
 // seed in scan order, `nseeds` the seeds present, `part` the full size of
 // the part; fills the remaining part - nseeds slots.
 static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint32_t start, int dir, uint32_t nseeds,
-                              uint32_t part, uint8_t c, uint32_t *runs, uint32_t *off, uint32_t *k0, uint32_t *v0,
-                              uint32_t *k1, uint32_t *v1, cudaStream_t s) {
-    if (nseeds == part) return PSACAK_OK;
+                              uint32_t part, uint8_t c, uint32_t *runs, uint32_t *off, uint8_t *endc, uint8_t *c0s,
+                              uint32_t *k0, uint64_t *v0, uint32_t *k1, uint64_t *v1, cudaStream_t s) {
+    if (part == 0) return PSACAK_OK;
     if (nseeds == 0 || nseeds > part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds for a part of %u", c, nseeds, part);
     uint32_t *d_max = ctx.d_scalars + 8;
     uint32_t *d_tot = ctx.d_scalars + 9;
     PSK_CUDA(cudaMemsetAsync(d_max, 0, sizeof(uint32_t), s));
     PSK_PROF_LAUNCH(s, "chain_runs", nseeds, 0,
-                    (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_max)));
-    PSK_LAUNCH_CHECK();
+                    (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_max,
+                                                                         c0s, endc)));
+    if (nseeds == part) return PSACAK_OK;
     PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(RunLoad{runs}, RunStore{off}, nseeds, ctx.d_partial, d_tot,
                                                    OpSum<uint32_t>(), ctx.scan_ctas, s)));
     uint32_t h[2];
@@ -264,13 +305,14 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     if (nseeds + ncells != part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds + %u chained != %u", c, nseeds, ncells, part);
     PSK_PROF_LAUNCH(s, "chain_expand", ncells, 0,
-                    (k_expand_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, ncells, k0, v0)));
+                    (k_expand_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, runs, endc, c,
+                                                                            ncells, k0, v0)));
     PSK_LAUNCH_CHECK();
     int in1 = 0;
-    PSK_TRY((ctx.radix_sort<uint32_t, uint32_t>(k0, v0, k1, v1, ncells, 0, bitlen(maxrun), &in1)));
+    PSK_TRY((ctx.radix_sort<uint32_t, uint64_t>(k0, v0, k1, v1, ncells, 0, bitlen(maxrun), &in1)));
     uint32_t first = dir > 0 ? start + nseeds : start - nseeds;
-    PSK_PROF_LAUNCH(s, "chain_place", ncells, 8ull * ncells,
-                    (k_place_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(in1 ? v1 : v0, ncells, first, dir, sa)));
+    PSK_PROF_LAUNCH(s, "chain_place", ncells, 13ull * ncells,
+                    (k_place_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(in1 ? v1 : v0, ncells, first, dir, sa, c0s)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -279,17 +321,19 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
 // cur[256..512) (the caller swaps the halves afterwards).
 template <bool LSCAN>
 static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t n, BucketSeq seq, uint8_t c,
-                           const uint32_t *cur_in, uint32_t *cur_out, cudaStream_t s, uint32_t *lms_out = nullptr,
-                           uint32_t lms_hi = 0, uint32_t lms_cap = 0) {
+                           const uint32_t *cur_in, uint32_t *cur_out, uint8_t *c0s, cudaStream_t s,
+                           uint32_t *lms_out = nullptr, uint32_t lms_hi = 0, uint32_t lms_cap = 0) {
     uint32_t nitems = seq.a_len + seq.b_len;
     if (nitems == 0) {
         PSK_CUDA(cudaMemcpyAsync(cur_out, cur_in, 256 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         return PSACAK_OK;
     }
     PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 8 * OS_BLOCK) + 1));
-    BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err, lms_out, lms_hi, lms_cap};
-    // algorithmic bytes: each entry read (4) and its predecessor's character
-    // (1); inducing entries written once (4, added from the device count).
+    BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err, lms_out, lms_hi, lms_cap,
+                            c0s};
+    // algorithmic bytes: each entry and its c0 read (5); inducing entries
+    // write entry + c0 (5, added from the device count) and read the text
+    // byte in front of their target (1, with it).
     return onesweep_ipt<BucketPolicy<LSCAN>>(pol, nitems, ctx.tile_ipt(), ctx.os, ctx.d_err, s, "induce_scatter",
                                               5ull * nitems);
 }
@@ -304,9 +348,13 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         maxpart = hg.lcount[c] > maxpart ? hg.lcount[c] : maxpart;
         maxpart = hg.scount[c] > maxpart ? hg.scount[c] : maxpart;
     }
-    DBuf<uint32_t> cur, cur2, runs, off, k0, v0, k1, v1;
+    DBuf<uint32_t> cur, cur2, runs, off, k0, k1;
+    DBuf<uint64_t> v0, v1;
+    DBuf<uint8_t> endc, c0s;
     PSK_TRY(cur.init(ctx, 512));
     PSK_TRY(cur2.init(ctx, 512));
+    PSK_TRY(endc.init(ctx, maxpart));
+    PSK_TRY(c0s.init(ctx, n));
     PSK_TRY(runs.init(ctx, maxpart));
     PSK_TRY(off.init(ctx, maxpart));
     PSK_TRY(k0.init(ctx, maxpart));
@@ -323,12 +371,14 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         const uint32_t G = ctx.scan_ctas;
         const uint64_t wchunk = ceil_div(nwords, G);
         PSK_PROF_LAUNCH(s, "place_lms", nwords, 0,
-                        (k_place_lms_any8<<<G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, wchunk)));
+                        (k_place_lms_any8<<<G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, c0s.get(),
+                                                                         wchunk)));
     } else if (n1 > 0) {
         PSK_PROF_LAUNCH(s, "place_lms", n1, 0,
-                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(text, sorted_lms, n1, dgeom, sa)));
+                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(text, sorted_lms, n1, dgeom, sa,
+                                                                                  c0s.get())));
     }
-    k_init_cursors<<<1, 256, 0, s>>>(dgeom, text, n, curL, curS, sa);
+    k_init_cursors<<<1, 256, 0, s>>>(dgeom, text, n, curL, curS, sa, c0s.get());
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
 
@@ -340,10 +390,11 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (lc > 0) {
             uint32_t cl = 0;
             PSK_TRY(ctx.read_u32(curL + c, &cl));
-            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, runs, off, k0, v0, k1, v1, s));
+            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, runs, off, endc, c0s, k0, v0, k1,
+                                  v1, s));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
-        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, s));
+        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, c0s, s));
         std::swap(curL, alt);
     }
     alt = cur2.get() + 256;
@@ -355,12 +406,12 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (sc > 0) {
             uint32_t cs = 0;
             PSK_TRY(ctx.read_u32(curS + c, &cs));
-            PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, runs, off, k0, v0, k1, v1,
-                                  s));
+            PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, runs, off, endc, c0s, k0, v0,
+                                  k1, v1, s));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
         const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;
-        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, s, extract ? lms_out : nullptr,
+        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, c0s, s, extract ? lms_out : nullptr,
                                   hg.lmsstart[c] + hg.lmscount[c] - 1, (uint32_t)n1));
         std::swap(curS, alt);
     }
