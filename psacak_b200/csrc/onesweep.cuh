@@ -51,6 +51,40 @@ __device__ __forceinline__ void os_store(uint64_t *p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Publishes this tile's count of digit d and returns the digit's exclusive
+// prefix over all earlier tiles: walks back over aggregates until a tile
+// with an inclusive prefix, then publishes its own inclusive prefix.  Each
+// poll of a not-yet-ready word counts against OS_SPIN_LIMIT.
+__device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile, uint32_t d, uint32_t count,
+                                                uint32_t epoch, uint32_t *err) {
+    uint64_t *my = status + (uint64_t)tile * 256 + d;
+    if (tile == 0) {
+        os_store(my, os_word(epoch, OS_FLAG_PREFIX, count));
+        return 0;
+    }
+    os_store(my, os_word(epoch, OS_FLAG_AGG, count));
+    uint32_t excl = 0;
+    int64_t t = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (t >= 0) {
+        uint64_t v = os_load(status + (uint64_t)t * 256 + d);
+        uint32_t ep = (uint32_t)(v >> 34);
+        uint64_t fl = (v >> 32) & 3ull;
+        if (ep != epoch || fl == 0) {
+            if (++spins > OS_SPIN_LIMIT) {
+                dev_fail(err, DEVERR_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        excl += (uint32_t)v;
+        if (fl == OS_FLAG_PREFIX) break;
+        t--;
+    }
+    os_store(my, os_word(epoch, OS_FLAG_PREFIX, excl + count));
+    return excl;
+}
+
 template <class Policy, int IPT>
 __global__ void __launch_bounds__(OS_BLOCK, Policy::kMinBlocks) k_onesweep(Policy pol, uint64_t n, uint64_t *status, uint32_t *ticket,
                                                        uint32_t epoch, uint32_t ntiles, uint32_t *err) {
@@ -108,34 +142,7 @@ __global__ void __launch_bounds__(OS_BLOCK, Policy::kMinBlocks) k_onesweep(Polic
         count += c;
     }
     s_tcount[d] = count;
-    // publish, then look back
-    uint64_t *my = status + (uint64_t)tile * 256 + d;
-    if (tile == 0) {
-        os_store(my, os_word(epoch, OS_FLAG_PREFIX, count));
-        s_excl[d] = 0;
-    } else {
-        os_store(my, os_word(epoch, OS_FLAG_AGG, count));
-        uint32_t excl = 0;
-        int64_t t = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        while (t >= 0) {
-            uint64_t v = os_load(status + (uint64_t)t * 256 + d);
-            uint32_t ep = (uint32_t)(v >> 34);
-            uint64_t fl = (v >> 32) & 3ull;
-            if (ep != epoch || fl == 0) {
-                if (++spins > OS_SPIN_LIMIT) {
-                    dev_fail(err, DEVERR_TIMEOUT);
-                    break;
-                }
-                continue;
-            }
-            excl += (uint32_t)v;
-            if (fl == OS_FLAG_PREFIX) break;
-            t--;
-        }
-        os_store(my, os_word(epoch, OS_FLAG_PREFIX, excl + count));
-        s_excl[d] = excl;
-    }
+    s_excl[d] = os_lookback(status, tile, d, count, epoch, err);
     uint32_t ex, tot;
     block_scan<uint32_t, OpSum<uint32_t>, OS_BLOCK>(count, OpSum<uint32_t>(), s_scan, &ex, &tot);
     s_tstart[d] = ex;

@@ -7,6 +7,7 @@
 #pragma once
 
 #include "onesweep.cuh"
+#include "tma.cuh"
 
 namespace psk {
 
@@ -40,6 +41,137 @@ template <class K, class V> struct RadixPolicy {
     }
     __device__ __forceinline__ void finish(uint32_t, uint32_t) const {}
 };
+
+// One radix pass as a TMA-fed onesweep tile.  A full tile's keys and values
+// arrive in shared memory by two bulk copies on an mbarrier (the ragged last
+// tile, or unaligned arrays, use plain loads), so no item is held in a
+// register while its load is in flight.  Items are ranked from shared
+// memory exactly as in k_onesweep (stable per-warp ranks, decoupled
+// look-back per digit), and the staging permutes 16-bit tile indices instead
+// of whole items: the scatter reads s_perm[i] and copies that item to
+// digit base + i, so consecutive threads write consecutive slots of a digit.
+// Shared memory: TILE * (sizeof(K) + sizeof(V) + 2) + 6.3 KB.
+constexpr int RS_MIN_BLOCKS = 4;
+
+template <class K, class V, int IPT>
+__global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
+    k_radix_pass(const K *__restrict__ kin, const V *__restrict__ vin, K *__restrict__ kout, V *__restrict__ vout,
+                 int shift, uint32_t dmask, const uint32_t *__restrict__ dbase, uint64_t n, int bulk_ok,
+                 uint64_t *status, uint32_t *ticket, uint32_t epoch, uint32_t *err) {
+    constexpr int TILE = OS_BLOCK * IPT;
+    extern __shared__ __align__(128) unsigned char rs_smem[];
+    K *s_k = (K *)rs_smem;
+    V *s_v = (V *)(s_k + TILE);
+    uint16_t *s_perm = (uint16_t *)(s_v + TILE);
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_gbase[256];
+    __shared__ uint32_t s_tstart[256];
+    __shared__ uint16_t s_wcnt[OS_WARPS][256];
+    __shared__ uint32_t s_scan[33];
+    __shared__ uint32_t s_tile;
+
+    const int w = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(ticket, 1u);
+        mbar_init(&s_bar, 1);
+    }
+    for (int i = threadIdx.x; i < OS_WARPS * 256; i += OS_BLOCK) (&s_wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * TILE;
+    const uint32_t cnt = (uint32_t)(n - base < (uint64_t)TILE ? n - base : (uint64_t)TILE);
+    const bool bulk = bulk_ok && cnt == (uint32_t)TILE;
+    if (bulk) {
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(&s_bar, TILE * (uint32_t)(sizeof(K) + sizeof(V)));
+            bulk_g2s(s_k, kin + base, TILE * (uint32_t)sizeof(K), &s_bar);
+            bulk_g2s(s_v, vin + base, TILE * (uint32_t)sizeof(V), &s_bar);
+        }
+        if (!mbar_wait_bounded(&s_bar, 0, err)) {
+            mbar_wait_bounded(&s_bar, 0, err);  // let the copies land before the CTA retires
+            return;
+        }
+    } else {
+        for (uint32_t i = threadIdx.x; i < cnt; i += OS_BLOCK) {
+            s_k[i] = kin[base + i];
+            s_v[i] = vin[base + i];
+        }
+        __syncthreads();
+    }
+
+    // stable ranks within the warp's sub-tile; packed (rank << 9 | digit)
+    uint32_t rd[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        const uint32_t idx = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
+        const uint32_t d = idx < cnt ? (uint32_t)(s_k[idx] >> shift) & dmask : 256u;
+        const uint32_t peers = __match_any_sync(FULL_MASK, d);
+        const uint32_t prior = d < 256 ? s_wcnt[w][d] : 0u;
+        rd[r] = ((prior + __popc(peers & lt)) << 9) | d;
+        __syncwarp();
+        if (d < 256 && (int)lane == __ffs(peers) - 1) s_wcnt[w][d] = (uint16_t)(prior + __popc(peers));
+        __syncwarp();
+    }
+    __syncthreads();
+    const uint32_t d = threadIdx.x;  // this thread's digit from here on
+    uint32_t count = 0;
+#pragma unroll
+    for (int ww = 0; ww < OS_WARPS; ww++) {
+        uint32_t c = s_wcnt[ww][d];
+        s_wcnt[ww][d] = (uint16_t)count;
+        count += c;
+    }
+    const uint32_t excl = os_lookback(status, tile, d, count, epoch, err);
+    uint32_t ex, tot;
+    block_scan<uint32_t, OpSum<uint32_t>, OS_BLOCK>(count, OpSum<uint32_t>(), s_scan, &ex, &tot);
+    s_tstart[d] = ex;
+    s_gbase[d] = dbase[d] + excl - ex;  // global slot of tile position i = s_gbase[digit] + i
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        const uint32_t dd = rd[r] & 511u;
+        if (dd < 256) {
+            const uint32_t idx = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
+            s_perm[s_tstart[dd] + s_wcnt[w][dd] + (rd[r] >> 9)] = (uint16_t)idx;
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += OS_BLOCK) {
+        const uint32_t li = s_perm[i];
+        const K k = s_k[li];
+        const uint64_t o = (uint64_t)s_gbase[(uint32_t)(k >> shift) & dmask] + i;
+        if (o < n) {
+            kout[o] = k;
+            vout[o] = s_v[li];
+        } else {
+            dev_fail(err, DEVERR_RANGE);
+        }
+    }
+}
+
+template <class K, class V, int IPT>
+status_t radix_pass(const K *kin, const V *vin, K *kout, V *vout, int shift, uint32_t dmask, const uint32_t *dbase,
+                    uint64_t n, OnesweepScratch &sc, uint32_t *err, cudaStream_t s) {
+    constexpr int TILE = OS_BLOCK * IPT;
+    const uint64_t ntiles = ceil_div(n, TILE);
+    if (ntiles > sc.max_tiles) return set_error(PSACAK_EINTERNAL, "radix pass: %llu tiles exceed scratch", (unsigned long long)ntiles);
+    if (TILE > 65536) return set_error(PSACAK_EINTERNAL, "radix pass: tile too large");
+    sc.epoch = (sc.epoch + 1) & ((1u << 30) - 1);
+    if (sc.epoch == 0) sc.epoch = 1;
+    uint32_t *ticket = sc.tickets + (sc.epoch & 63);
+    PSK_CUDA(cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s));
+    const int bulk_ok = ((((uintptr_t)kin) | ((uintptr_t)vin)) & 15u) == 0;
+    const size_t smem = (size_t)TILE * (sizeof(K) + sizeof(V) + 2);
+    PSK_CUDA(cudaFuncSetAttribute(k_radix_pass<K, V, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PSK_PROF_LAUNCH(s, "radix_pass", n, 2 * n * (sizeof(K) + sizeof(V)),
+                    (k_radix_pass<K, V, IPT><<<(uint32_t)ntiles, OS_BLOCK, smem, s>>>(
+                        kin, vin, kout, vout, shift, dmask, dbase, n, bulk_ok, sc.status, ticket, sc.epoch, err)));
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
 
 // Digit counts of every pass: hist[p * 256 + d].
 template <class K>
@@ -102,9 +234,14 @@ status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit,
         if (trivial) continue;
         int shift = begin_bit + 8 * p;
         int bits = end_bit - shift < 8 ? end_bit - shift : 8;
-        RadixPolicy<K, V> pol{ki, vi, ko, vo, shift, (1u << bits) - 1, bases + p * 256};
-        PSK_TRY((onesweep_ipt<RadixPolicy<K, V>>(pol, n, ipt, sc, err, s, "radix_pass",
-                                                 2 * n * (sizeof(K) + sizeof(V)))));
+        const uint32_t dmask = (1u << bits) - 1;
+        if (ipt == 8) {
+            PSK_TRY((radix_pass<K, V, 8>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s)));
+        } else if (ipt == 16) {
+            PSK_TRY((radix_pass<K, V, 16>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s)));
+        } else {
+            PSK_TRY((radix_pass<K, V, 12>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s)));
+        }
         K *tk = ki; ki = ko; ko = tk;
         V *tv = vi; vi = vo; vo = tv;
         flip ^= 1;

@@ -65,6 +65,20 @@ def test_radix_sort_u64(st, n, b0, b1):
     assert (dk.cpu().numpy().view(np.uint64) == keys[order]).all()
 
 
+@pytest.mark.parametrize("n", [3071, 3072, 300_001])
+def test_radix_sort_u64_unaligned(st, n):
+    """Arrays that are not 16-byte aligned take the plain-load path of the
+    radix pass instead of the bulk copies."""
+    rng = np.random.default_rng(n + 5)
+    keys = rng.integers(0, 2**40, n + 1, dtype=np.int64).astype(np.uint64)
+    vals = np.arange(n + 1, dtype=np.uint32)
+    order = np.argsort(keys[1:], kind="stable")
+    dk, dv = dev(keys.view(np.int64)), dev(vals.view(np.int32))
+    st.radix_sort_u64(dk[1:].data_ptr(), dv[1:].data_ptr(), n, 0, 40)
+    assert (dv[1:].cpu().numpy().view(np.uint32) == vals[1:][order]).all()
+    assert (dk[1:].cpu().numpy().view(np.uint64) == keys[1:][order]).all()
+
+
 @pytest.mark.parametrize("n", [1, 7, 4096, 4097, 1_000_000, 5_000_001])
 def test_radix_sort_u32(st, n):
     rng = np.random.default_rng(n + 1)
