@@ -46,7 +46,7 @@ typedef struct {
     uint32_t inner_engine;     /* PSACAK_ENGINE_* for levels >= 1 */
     uint32_t scan_ctas_per_sm; /* CTAs per SM of the chunked scans (0 = 4) */
     uint32_t batch_chunk_mib;  /* batch builds: max MiB per concatenated build (0 = 3072) */
-    uint32_t tile_items;       /* items per thread of the single-pass scatter: 8, 12 or 16 (0 = 12) */
+    uint32_t tile_items;       /* items per thread of the bucket scatter and compactions: 8, 12 or 16 (0 = 8) */
     uint32_t finish_below;     /* recursion strategy: integer levels shorter than this are sorted
                                   directly by prefix doubling instead of recursing (0 = never) */
     uint32_t reserved[2];

@@ -43,10 +43,19 @@ __global__ void k_hash_u32(const uint32_t *__restrict__ v, uint64_t n, unsigned 
 }
 
 // S-type counts of translated buckets: scnt[text[j]] += 1 for S positions.
+// Lanes holding the same symbol share one atomic (frequent symbols would
+// otherwise serialise on their counter).
 __global__ void k_count_s(const uint32_t *__restrict__ text, uint64_t n, const uint32_t *__restrict__ types,
                           uint32_t *scnt) {
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
-        if (bm_get(types, j)) atomicAdd(&scnt[text[j]], 1u);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t jb = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); jb < n; jb += stride) {
+        const uint64_t j = jb + lane;
+        const bool s = j < n && bm_get(types, j);
+        const uint32_t v = s ? text[j] : 0xFFFFFFFFu;
+        const uint32_t peers = __match_any_sync(FULL_MASK, v);
+        if (s && (int)lane == __ffs(peers) - 1) atomicAdd(&scnt[v], __popc(peers));
+    }
 }
 
 struct SortedLmsPred {

@@ -132,10 +132,11 @@ struct Ctx {
         if (stage_t0 > 0) fprintf(stderr, "[psacak] level %u %-24s %9.3f ms\n", level, what, t - stage_t0);
         stage_t0 = t;
     }
-    // Items per thread of the single-pass scatter (schedule tile_items).
+    // Items per thread of the bucket scans' scatter and of the compactions
+    // (schedule tile_items; 0 = 8).  Radix passes always use RADIX_IPT.
     int tile_ipt() const {
         uint32_t t = sched.tile_items;
-        return (t == 8 || t == 16) ? (int)t : 12;
+        return (t == 12 || t == 16) ? (int)t : 8;
     }
     // Grows the onesweep status array to hold `tiles` tiles.
     status_t ensure_onesweep(uint64_t tiles) {
@@ -155,7 +156,7 @@ struct Ctx {
     template <class K, class V>
     status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1) {
         PSK_TRY(ensure_onesweep(ceil_div(n, 8 * OS_BLOCK) + 1));
-        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream, tile_ipt());
+        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream, RADIX_IPT);
     }
     // Single-pass stable compaction (see compact1).
     template <class Pred, class Emit>

@@ -53,36 +53,55 @@ struct BucketSeq {
 
 // LMS-substring mode placement: LMS positions go to the tail of their bucket
 // in arbitrary order.  Each CTA walks a contiguous range of 32-position words
-// (a warp per word, a lane per position, so the text is read coalesced),
-// counts its LMS per character in shared memory, reserves one range per
-// character with a single global atomic, then writes into it.
+// (a warp per word, a lane per position, so the text is read coalesced;
+// PL_UNROLL words per warp step so that their loads overlap), counts its LMS
+// per character in shared memory, reserves one range per character with a
+// single global atomic, then writes into it.
 constexpr int PL_BLOCK = 256;
+constexpr int PL_WARPS = PL_BLOCK / 32;
+constexpr int PL_UNROLL = 4;
 __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__restrict__ text, uint64_t nwords,
                                                              const uint32_t *__restrict__ lms,
                                                              const ByteGeom *__restrict__ g, uint32_t *cursor,
                                                              uint32_t *sa, uint8_t *c0s, uint64_t wchunk) {
-    __shared__ uint32_t s_cnt[256], s_base[256];
+    __shared__ uint32_t s_cnt[256], s_base[256], s_tail[256];
     s_cnt[threadIdx.x] = 0;
+    s_tail[threadIdx.x] = g->tail[threadIdx.x];
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, lt = lanemask_lt();
     const uint64_t w0 = (uint64_t)blockIdx.x * wchunk;
     const uint64_t w1 = w0 + wchunk < nwords ? w0 + wchunk : nwords;
     for (int pass = 0; pass < 2; pass++) {
-        for (uint64_t w = w0 + warp; w < w1; w += PL_BLOCK / 32) {
-            uint32_t word = lms[w];
-            if (!word) continue;
-            bool on = (word >> lane) & 1u;
-            uint32_t c = on ? text[(w << 5) + lane] : 256u;
-            uint32_t peers = __match_any_sync(FULL_MASK, c);
-            int leader = __ffs(peers) - 1;
-            uint32_t got = 0;
-            if (on && (int)lane == leader) got = atomicAdd(&s_cnt[c], __popc(peers));
-            got = __shfl_sync(FULL_MASK, got, leader);
-            if (pass == 1 && on) {
-                const uint32_t slot = g->tail[c] - 1 - (s_base[c] + got + __popc(peers & lt));
-                const uint64_t p = (w << 5) + lane;  // LMS positions are > 0
-                sa[slot] = (uint32_t)p;
-                c0s[slot] = text[p - 1];
+        for (uint64_t wb = w0 + warp; wb < w1; wb += PL_WARPS * PL_UNROLL) {
+            uint32_t word[PL_UNROLL], c[PL_UNROLL];
+            uint8_t pc[PL_UNROLL];
+#pragma unroll
+            for (int u = 0; u < PL_UNROLL; u++) {
+                const uint64_t w = wb + (uint64_t)u * PL_WARPS;
+                word[u] = w < w1 ? lms[w] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < PL_UNROLL; u++) {
+                const uint64_t p = ((wb + (uint64_t)u * PL_WARPS) << 5) + lane;  // LMS positions are > 0
+                const bool on = (word[u] >> lane) & 1u;
+                c[u] = on ? text[p] : 256u;
+                pc[u] = (pass == 1 && on) ? text[p - 1] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < PL_UNROLL; u++) {
+                if (!word[u]) continue;  // warp-uniform
+                const uint32_t cc = c[u];
+                const bool on = cc < 256;
+                const uint32_t peers = __match_any_sync(FULL_MASK, cc);
+                const int leader = __ffs(peers) - 1;
+                uint32_t got = 0;
+                if (on && (int)lane == leader) got = atomicAdd(&s_cnt[cc], __popc(peers));
+                got = __shfl_sync(FULL_MASK, got, leader);
+                if (pass == 1 && on) {
+                    const uint32_t slot = s_tail[cc] - 1 - (s_base[cc] + got + __popc(peers & lt));
+                    sa[slot] = (uint32_t)(((wb + (uint64_t)u * PL_WARPS) << 5) + lane);
+                    c0s[slot] = pc[u];
+                }
             }
         }
         __syncthreads();
@@ -95,14 +114,40 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
     }
 }
 
-__global__ void k_place_lms_sorted8(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sorted,
-                                    uint64_t n1, const ByteGeom *__restrict__ g, uint32_t *sa, uint8_t *c0s) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t p = sorted[i];
-        uint8_t c = text[p];
-        uint32_t slot = g->tail[c] - g->lmscount[c] + ((uint32_t)i - g->lmsstart[c]);
-        sa[slot] = p;
-        c0s[slot] = text[p - 1];
+// Final mode placement: the sorted LMS suffixes fill the tail of each
+// bucket in order.  Four entries per thread step so their text gathers
+// overlap; the bucket geometry is read from shared memory.
+constexpr int PS_UNROLL = 4;
+__global__ void __launch_bounds__(256) k_place_lms_sorted8(const uint8_t *__restrict__ text,
+                                                           const uint32_t *__restrict__ sorted, uint64_t n1,
+                                                           const ByteGeom *__restrict__ g, uint32_t *sa,
+                                                           uint8_t *c0s) {
+    __shared__ uint32_t s_off[256];  // slot of list entry i = s_off[c] + i
+    s_off[threadIdx.x] = g->tail[threadIdx.x] - g->lmscount[threadIdx.x] - g->lmsstart[threadIdx.x];
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n1; i0 += stride * PS_UNROLL) {
+        uint32_t p[PS_UNROLL];
+        uint8_t c[PS_UNROLL], pc[PS_UNROLL];
+#pragma unroll
+        for (int u = 0; u < PS_UNROLL; u++) {
+            const uint64_t i = i0 + (uint64_t)u * stride;
+            p[u] = i < n1 ? sorted[i] : 1u;
+        }
+#pragma unroll
+        for (int u = 0; u < PS_UNROLL; u++) {
+            c[u] = text[p[u]];
+            pc[u] = text[p[u] - 1];  // LMS positions are > 0
+        }
+#pragma unroll
+        for (int u = 0; u < PS_UNROLL; u++) {
+            const uint64_t i = i0 + (uint64_t)u * stride;
+            if (i < n1) {
+                const uint32_t slot = s_off[c[u]] + (uint32_t)i;
+                sa[slot] = p[u];
+                c0s[slot] = pc[u];
+            }
+        }
     }
 }
 
@@ -368,10 +413,10 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
     if (mode == INDUCE_LMS_SUBSTRINGS) {
         PSK_CUDA(cudaMemsetAsync(curL, 0, 256 * sizeof(uint32_t), s));
         const uint64_t nwords = ceil_div(n, 32);
-        const uint32_t G = ctx.scan_ctas;
+        const uint64_t G = ceil_div(nwords, 2048) < 4ull * ctx.scan_ctas ? ceil_div(nwords, 2048) : 4ull * ctx.scan_ctas;
         const uint64_t wchunk = ceil_div(nwords, G);
         PSK_PROF_LAUNCH(s, "place_lms", nwords, 0,
-                        (k_place_lms_any8<<<G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, c0s.get(),
+                        (k_place_lms_any8<<<(uint32_t)G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, c0s.get(),
                                                                          wchunk)));
     } else if (n1 > 0) {
         PSK_PROF_LAUNCH(s, "place_lms", n1, 0,

@@ -56,19 +56,34 @@ struct OpTri {
 
 // LMS-substring mode: LMS positions take distinct slots at the tail of their
 // bucket in arbitrary order (the reference's put_lmscharacters,
-// src/psacak8.rs:57-72 / src/psacak32.rs:60-99).
+// src/psacak8.rs:57-72 / src/psacak32.rs:60-99).  A lane per 32-position
+// word; lanes that meet the same bucket in one step share one atomic
+// (frequent symbols would otherwise serialise on their cursor).
 template <class C>
 __global__ void k_place_lms_any(const C *__restrict__ text, uint64_t nwords, const uint32_t *__restrict__ lms,
                                 Geom<C> g, uint32_t *cursor, uint32_t *R) {
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t word = lms[w];
-        while (word) {
-            int b = __ffs(word) - 1;
-            word &= word - 1;
-            uint64_t p = (w << 5) + b;
-            C c = text[p];
-            uint32_t slot = atomicAdd(&cursor[g.bucket(c)], 1u);
-            R[p] = g.tail(c) - slot;  // slot tail-1-slot, plus one
+    const uint32_t lane = threadIdx.x & 31, lt = lanemask_lt();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t wb = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); wb < nwords; wb += stride) {
+        const uint64_t w = wb + lane;
+        uint32_t word = w < nwords ? lms[w] : 0u;
+        while (__any_sync(FULL_MASK, word != 0)) {
+            const bool on = word != 0;
+            uint64_t p = 0;
+            C c = 0;
+            uint32_t bk = 0xFFFFFFFFu;
+            if (on) {
+                p = (w << 5) + (uint64_t)(__ffs(word) - 1);
+                word &= word - 1;
+                c = text[p];
+                bk = g.bucket(c);
+            }
+            const uint32_t peers = __match_any_sync(FULL_MASK, bk);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (on && (int)lane == leader) base = atomicAdd(&cursor[bk], __popc(peers));
+            base = __shfl_sync(FULL_MASK, base, leader);
+            if (on) R[p] = g.tail(c) - (base + __popc(peers & lt));  // slot tail-1-rank, plus one
         }
     }
 }

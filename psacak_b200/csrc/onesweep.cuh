@@ -25,6 +25,8 @@
 //   store(index, item, digit)
 //   finish(digit, total)            -> called once per digit by the last tile
 //   kMinBlocks                      -> CTAs per SM the register budget must allow
+//                                      at 12 items per thread (raised by
+//                                      12 / IPT for smaller tiles)
 #pragma once
 
 #include "prims.cuh"
@@ -85,8 +87,10 @@ __device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile,
     return excl;
 }
 
+constexpr int os_min_blocks(int at12, int ipt) { return ipt < 12 ? at12 * 12 / ipt : at12; }
+
 template <class Policy, int IPT>
-__global__ void __launch_bounds__(OS_BLOCK, Policy::kMinBlocks) k_onesweep(Policy pol, uint64_t n, uint64_t *status, uint32_t *ticket,
+__global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IPT)) k_onesweep(Policy pol, uint64_t n, uint64_t *status, uint32_t *ticket,
                                                        uint32_t epoch, uint32_t ntiles, uint32_t *err) {
     using Item = typename Policy::Item;
     constexpr int TILE = OS_BLOCK * IPT;

@@ -52,6 +52,7 @@ template <class K, class V> struct RadixPolicy {
 // digit base + i, so consecutive threads write consecutive slots of a digit.
 // Shared memory: TILE * (sizeof(K) + sizeof(V) + 2) + 6.3 KB.
 constexpr int RS_MIN_BLOCKS = 4;
+constexpr int RADIX_IPT = 12;  // items per thread of the radix passes (3072-item tiles)
 
 template <class K, class V, int IPT>
 __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)

@@ -26,7 +26,7 @@ SCHEDULES = [
     {"engine": e, "inner_engine": ENGINE_DOUBLING, "tile_items": t, "finish_below": f}
     for e in (ENGINE_BUCKET, ENGINE_DOUBLING) for t in (8, 12, 16) for f in (0, 1 << 16)
 ]
-DEFAULT_INDEX = SCHEDULES.index({"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 12,
+DEFAULT_INDEX = SCHEDULES.index({"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 8,
                                  "finish_below": 0})
 
 
