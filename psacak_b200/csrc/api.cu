@@ -153,9 +153,11 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         PSK_TRY(dgeom.init(ctx, 1));
     }
     ctx.mark("enter", level);
-    PSK_TRY(type_text<C>(text, n, types, lms, wcnt, bytes ? hist.get() : nullptr, tscratch, ctx.scan_ctas, s));
+    PSK_TRY(ctx.ensure_scan(n));
+    const ScanEnv env = ctx.scan_env();
+    PSK_TRY(type_text<C>(text, n, types, lms, wcnt, bytes ? hist.get() : nullptr, tscratch, env, ctx.scan_ctas, s));
     tscratch.reset();
-    PSK_TRY(lms_prefix(wcnt, nwords, pref, ctx.d_partial, ctx.d_scalars, ctx.scan_ctas, s));
+    PSK_TRY(lms_prefix(wcnt, nwords, pref, ctx.d_scalars, env, s));
     wcnt.reset();
     uint32_t n1u = 0;
     PSK_TRY(ctx.read_u32(ctx.d_scalars, &n1u));
@@ -245,8 +247,8 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         PSK_TRY(red.init(ctx, n1));
         PSK_TRY(heads.init(ctx, n1 + 1));
         PSK_TRY(flags.init(ctx, n1));
-        PSK_TRY(name_lms<C>(text, n, lms, pref, sorted, n1, red, heads, flags, ctx.d_partial, ctx.d_scalars + 2,
-                            ctx.scan_ctas, s));
+        PSK_TRY(name_lms<C>(text, n, lms, pref, sorted, n1, red, heads, flags, ctx.d_scalars + 2, env, ctx.scan_ctas,
+                            s));
         PSK_TRY(ctx.read_u32(ctx.d_scalars + 2, &k));
     }
     sorted.reset();
@@ -262,7 +264,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
                 PSK_TRY(l1.init(ctx, w1 + 1));
                 PSK_TRY(c1.init(ctx, w1 + 1));
                 PSK_TRY(sc1.init(ctx, 2 * ceil_div(n1, TYPE_TILE) + 1024));
-                PSK_TRY(type_text<uint32_t>(red, n1, t1, l1, c1, nullptr, sc1, ctx.scan_ctas, s));
+                PSK_TRY(type_text<uint32_t>(red, n1, t1, l1, c1, nullptr, sc1, env, ctx.scan_ctas, s));
                 // the names stay as the next level's dense bucket ids
                 PSK_TRY(names1.init(ctx, n1));
                 PSK_CUDA(cudaMemcpyAsync(names1.get(), red.get(), n1 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -420,8 +422,8 @@ status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa
     const uint32_t *pos = in1 ? v1.get() : v0.get();
     DBuf<uint32_t> names;
     PSK_TRY(names.init(ctx, n));
-    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(DistinctLoad{vals}, RankStore{pos, names}, n, ctx.d_partial,
-                                                   ctx.d_scalars + 3, OpSum<uint32_t>(), ctx.scan_ctas, s)));
+    PSK_TRY((ctx.scan<uint32_t, OpSum<uint32_t>>(DistinctLoad{vals}, RankStore{pos, names}, n, ctx.d_scalars + 3,
+                                                 OpSum<uint32_t>(), "scan_ranks")));
     uint32_t distinct = 0;
     PSK_TRY(ctx.read_u32(ctx.d_scalars + 3, &distinct));
     if (distinct >= n) {
@@ -438,14 +440,14 @@ status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa
     PSK_TRY(lms.init(ctx, nwords + 1));
     PSK_TRY(wcnt.init(ctx, nwords + 1));
     PSK_TRY(tscratch.init(ctx, 2 * ceil_div(n, TYPE_TILE) + 1024));
-    PSK_TRY(type_text<uint32_t>(text, n, types, lms, wcnt, nullptr, tscratch, ctx.scan_ctas, s));
+    PSK_TRY(ctx.ensure_scan(n));
+    PSK_TRY(type_text<uint32_t>(text, n, types, lms, wcnt, nullptr, tscratch, ctx.scan_env(), ctx.scan_ctas, s));
     PSK_TRY(head.init(ctx, n));
     PSK_TRY(t2.init(ctx, n));
-    PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(HeadLoad{vals}, HeadStore{head}, n, ctx.d_partial,
-                                                   (uint32_t *)nullptr, OpMax<uint32_t>(), ctx.scan_ctas, s)));
-    PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(TailLoad{vals, n}, TailStore{vals, pos, head, types, n, t2}, n,
-                                                   ctx.d_partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
-                                                   ctx.scan_ctas, s)));
+    PSK_TRY((ctx.scan<uint32_t, OpMax<uint32_t>>(HeadLoad{vals}, HeadStore{head}, n, (uint32_t *)nullptr,
+                                                 OpMax<uint32_t>(), "scan_heads")));
+    PSK_TRY((ctx.scan<uint32_t, OpMax<uint32_t>>(TailLoad{vals, n}, TailStore{vals, pos, head, types, n, t2}, n,
+                                                 (uint32_t *)nullptr, OpMax<uint32_t>(), "scan_tails")));
     types.reset();
     lms.reset();
     wcnt.reset();
@@ -458,8 +460,7 @@ status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa
     // bucket boundaries by symbol rank
     DBuf<uint32_t> bheads;
     PSK_TRY(bheads.init(ctx, (uint64_t)distinct + 1));
-    PSK_TRY(compact(DistinctPred{vals, n}, HeadEmit{bheads, n, distinct}, n + 1, ctx.d_partial, (uint32_t *)nullptr,
-                    ctx.scan_ctas, s));
+    PSK_TRY(ctx.compact(DistinctPred{vals, n}, HeadEmit{bheads, n, distinct}, n + 1, ctx.d_scalars + 5, "bucket_heads"));
     return build_level<uint32_t>(ctx, t2, names, bheads, distinct, n, sa, 0);
 }
 
@@ -478,7 +479,6 @@ status_t ctx_init(Ctx &c, int device) {
     PSK_CUDA(cudaMallocHost(&c.h_pinned, 4096));
     PSK_CUDA(cudaMallocHost(&c.h_hist, RADIX_MAX_PASSES * 256 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.os.tickets, 64 * sizeof(uint32_t)));
-    PSK_CUDA(cudaMalloc(&c.d_partial, MAX_CHUNKS * 4 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_hist, 256 * RADIX_MAX_CTAS * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_err, sizeof(uint32_t)));
@@ -498,9 +498,13 @@ void ctx_free(Ctx &c) {
     if (c.os.tickets) cudaFree(c.os.tickets);
     if (c.os.status) cudaFree(c.os.status);
     c.os.status = nullptr;
+    if (c.ss.flags) cudaFree(c.ss.flags);
+    if (c.ss.vals) cudaFree(c.ss.vals);
+    c.ss.flags = nullptr;
+    c.ss.vals = nullptr;
+    c.ss.max_tiles = 0;
     c.os.tickets = nullptr;
     c.h_hist = nullptr;
-    if (c.d_partial) cudaFree(c.d_partial);
     if (c.d_hist) cudaFree(c.d_hist);
     if (c.d_scalars) cudaFree(c.d_scalars);
     if (c.d_err) cudaFree(c.d_err);
@@ -917,8 +921,8 @@ int psacak_debug_exclusive_sum(psacak_ctx *ctx, const uint32_t *d_in, uint32_t *
     Ctx &c = ctx->c;
     PSK_CUDA(cudaSetDevice(c.dev.id));
     c.stream = c.own_stream;
-    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(CopyLoad{d_in}, CopyStore{d_out}, n, c.d_partial,
-                                                   (uint32_t *)nullptr, OpSum<uint32_t>(), c.scan_ctas, c.stream)));
+    PSK_TRY((c.scan<uint32_t, OpSum<uint32_t>>(CopyLoad{d_in}, CopyStore{d_out}, n, (uint32_t *)nullptr,
+                                               OpSum<uint32_t>(), "scan")));
     return c.sync();
 }
 
@@ -935,11 +939,13 @@ int psacak_debug_types(psacak_ctx *ctx, const void *d_text, uint64_t n, int widt
     PSK_TRY(wcnt.init(c, ceil_div(n, 32) + 1));
     PSK_TRY(scr.init(c, 2 * ceil_div(n, TYPE_TILE) + 1024));
     PSK_TRY(hist.init(c, 1));
+    PSK_TRY(c.ensure_scan(n));
     if (width == 1)
-        PSK_TRY(type_text<uint8_t>((const uint8_t *)d_text, n, d_types, d_lms, wcnt, hist, scr, c.scan_ctas, c.stream));
+        PSK_TRY(type_text<uint8_t>((const uint8_t *)d_text, n, d_types, d_lms, wcnt, hist, scr, c.scan_env(),
+                                   c.scan_ctas, c.stream));
     else
-        PSK_TRY(type_text<uint32_t>((const uint32_t *)d_text, n, d_types, d_lms, wcnt, nullptr, scr, c.scan_ctas,
-                                    c.stream));
+        PSK_TRY(type_text<uint32_t>((const uint32_t *)d_text, n, d_types, d_lms, wcnt, nullptr, scr, c.scan_env(),
+                                    c.scan_ctas, c.stream));
     return c.sync();
 }
 

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <vector>
 
+#include "level.cuh"
 #include "radix.cuh"
 
 struct psacak_ctx;
@@ -20,13 +21,13 @@ struct Ctx {
     cudaStream_t stream = nullptr;  // stream of the current call
     cudaMemPool_t pool = nullptr;
     uint32_t *h_pinned = nullptr;   // small pinned buffer for scalar read-backs
-    uint32_t *d_partial = nullptr;  // MAX_CHUNKS * 4 uint32 scan partials
     uint32_t *d_hist = nullptr;     // 256 * RADIX_MAX_CTAS radix histograms
     uint32_t *d_scalars = nullptr;  // 64 device scalars
     uint32_t *d_err = nullptr;      // device error word
     uint32_t *h_hist = nullptr;     // pinned copy of the radix digit counts
     OnesweepScratch os;             // look-back status words of the onesweep kernels
-    uint32_t scan_ctas = 0;         // CTAs of the chunked scans
+    ScanScratch ss;                 // look-back flags and values of the single-pass scans
+    uint32_t scan_ctas = 0;         // CTAs of the grid-stride helper kernels
     uint32_t radix_ctas = 0;        // CTAs of the radix passes
     psacak_schedule sched{};
     // When set, level 0 stops after building its reduced string and copies
@@ -150,6 +151,30 @@ struct Ctx {
         PSK_CUDA(cudaMemsetAsync(os.status, 0, want * 256 * sizeof(uint64_t), stream));
         os.max_tiles = want;
         return PSACAK_OK;
+    }
+    // Grows the single-pass scan scratch to cover `n` items.
+    status_t ensure_scan(uint64_t n) {
+        const uint64_t tiles = ceil_div(n ? n : 1, LS_TILE_MIN) + 1;
+        if (tiles <= ss.max_tiles) return PSACAK_OK;
+        const uint64_t want = tiles + tiles / 4 + 64;
+        if (ss.flags) cudaFreeAsync(ss.flags, stream);
+        if (ss.vals) cudaFreeAsync(ss.vals, stream);
+        ss.flags = nullptr;
+        ss.vals = nullptr;
+        ss.max_tiles = 0;
+        PSK_CUDA(cudaMallocAsync(&ss.flags, want * sizeof(uint64_t), stream));
+        PSK_CUDA(cudaMallocAsync(&ss.vals, want * 2 * LS_MAX_VALUE_BYTES, stream));
+        // zeroed flags read as "not ready" for every epoch
+        PSK_CUDA(cudaMemsetAsync(ss.flags, 0, want * sizeof(uint64_t), stream));
+        ss.max_tiles = want;
+        return PSACAK_OK;
+    }
+    ScanEnv scan_env() { return ScanEnv{&ss, &os, d_err}; }
+    // Single-pass scan (see lbscan.cuh) over n items.
+    template <class T, class Op, class Load, class Store>
+    status_t scan(Load ld, Store st, uint64_t n, T *total_out, Op op, const char *name) {
+        PSK_TRY(ensure_scan(n));
+        return lb_scan<T, Op>(ld, st, n, total_out, op, ss, os, d_err, stream, name);
     }
     // Stable LSD radix sort of (key, value) pairs on bits [b0, b1); the
     // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).

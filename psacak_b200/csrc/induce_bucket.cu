@@ -342,8 +342,8 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
                     (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_max,
                                                                          c0s, endc)));
     if (nseeds == part) return PSACAK_OK;
-    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(RunLoad{runs}, RunStore{off}, nseeds, ctx.d_partial, d_tot,
-                                                   OpSum<uint32_t>(), ctx.scan_ctas, s)));
+    PSK_TRY((ctx.scan<uint32_t, OpSum<uint32_t>>(RunLoad{runs}, RunStore{off}, nseeds, d_tot, OpSum<uint32_t>(),
+                                                 "scan_runs")));
     uint32_t h[2];
     PSK_TRY(ctx.read_u32(d_max, h, 2));
     const uint32_t maxrun = h[0], ncells = h[1];

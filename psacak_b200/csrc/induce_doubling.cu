@@ -278,9 +278,9 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
         PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, &in1)));
         const uint64_t *ks = in1 ? k1 : k0;
         const uint32_t *vs = in1 ? v1 : v0;
-        PSK_TRY((chunk_scan<Tri, OpTri>(RoundLoad{ks, cnt, KB},
-                                        RoundStore{ks, vs, KB, gA, gB, R, sa, Wg, Wv, n, ngroups, ctx.d_err}, cnt,
-                                        (Tri *)ctx.d_partial, d_tri, OpTri(), ctx.scan_ctas, s)));
+        PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, cnt, KB},
+                                      RoundStore{ks, vs, KB, gA, gB, R, sa, Wg, Wv, n, ngroups, ctx.d_err}, cnt, d_tri,
+                                      OpTri(), "scan_rounds")));
         uint32_t tri[4];
         PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
         if (ctx.stage_timing)
@@ -319,10 +319,9 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
                                                                                             cursor, R)));
         PSK_LAUNCH_CHECK();
     } else if (n1 > 0) {
-        PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{text, sorted_lms, n1, geom},
-                                                       LastStore<C>{text, sorted_lms, n1, geom, R}, n1,
-                                                       ctx.d_partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
-                                                       ctx.scan_ctas, s)));
+        PSK_TRY((ctx.scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{text, sorted_lms, n1, geom},
+                                                     LastStore<C>{text, sorted_lms, n1, geom, R}, n1,
+                                                     (uint32_t *)nullptr, OpMax<uint32_t>(), "scan_last")));
     }
     PSK_TRY((doubling_scan<C, false>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));
     PSK_TRY((doubling_scan<C, true>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));

@@ -175,17 +175,16 @@ __global__ void __launch_bounds__(TYPE_BLOCK) k_type_main(const C *__restrict__ 
 
 template <class C>
 status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, uint32_t *lms_wcnt,
-                   ByteHist *hist, uint32_t *scratch, uint32_t max_ctas, cudaStream_t s) {
+                   ByteHist *hist, uint32_t *scratch, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s) {
     if (n == 0) return PSACAK_OK;
     uint64_t ntiles = ceil_div(n, TYPE_TILE);
     uint32_t *code = scratch;
     uint32_t *carry = scratch + ntiles;
-    uint32_t *partial = scratch + 2 * ntiles;
     uint32_t grid = (uint32_t)(ntiles < max_ctas ? ntiles : max_ctas);
     PSK_PROF_LAUNCH(s, "type_tile_first", ntiles, 0, (k_tile_first<C><<<grid, TYPE_BLOCK, 0, s>>>(text, n, ntiles, code)));
-    PSK_TRY((chunk_scan<uint32_t, OpMax<uint32_t>>(TileCarryLoad{code, ntiles}, TileCarryStore{carry, ntiles},
-                                                   ntiles, partial, (uint32_t *)nullptr, OpMax<uint32_t>(),
-                                                   max_ctas, s)));
+    PSK_TRY((lb_scan<uint32_t, OpMax<uint32_t>>(TileCarryLoad{code, ntiles}, TileCarryStore{carry, ntiles}, ntiles,
+                                                (uint32_t *)nullptr, OpMax<uint32_t>(), *env.ss, *env.os, env.err, s,
+                                                "scan_tile_carry")));
     // algorithmic bytes: the text once, two bitmaps and the word counts
     const uint64_t tbytes = n * sizeof(C) + 3 * ceil_div(n, 32) * 4;
     if (hist) {
@@ -203,9 +202,9 @@ status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, ui
 }
 
 template status_t type_text<uint8_t>(const uint8_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, ByteHist *,
-                                     uint32_t *, uint32_t, cudaStream_t);
+                                     uint32_t *, const ScanEnv &, uint32_t, cudaStream_t);
 template status_t type_text<uint32_t>(const uint32_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, ByteHist *,
-                                      uint32_t *, uint32_t, cudaStream_t);
+                                      uint32_t *, const ScanEnv &, uint32_t, cudaStream_t);
 
 struct PrefLoad {
     const uint32_t *w;
@@ -218,10 +217,10 @@ struct PrefStore {
 
 __global__ void k_copy_total(const uint32_t *total, uint32_t *dst) { *dst = *total; }
 
-status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *partial,
-                    uint32_t *total, uint32_t max_ctas, cudaStream_t s) {
-    PSK_TRY((chunk_scan<uint32_t, OpSum<uint32_t>>(PrefLoad{lms_wcnt}, PrefStore{pref}, nwords, partial, total,
-                                                   OpSum<uint32_t>(), max_ctas, s)));
+status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *total,
+                    const ScanEnv &env, cudaStream_t s) {
+    PSK_TRY((lb_scan<uint32_t, OpSum<uint32_t>>(PrefLoad{lms_wcnt}, PrefStore{pref}, nwords, total, OpSum<uint32_t>(),
+                                                *env.ss, *env.os, env.err, s, "scan_lms_prefix")));
     k_copy_total<<<1, 1, 0, s>>>(total, pref + nwords);
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
@@ -291,7 +290,7 @@ struct NameStore {
 template <class C>
 status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t *lms_pref,
                   const uint32_t *sorted, uint64_t n1, uint32_t *red, uint32_t *heads, uint32_t *flags,
-                  uint32_t *partial, uint32_t *k_out, uint32_t max_ctas, cudaStream_t s) {
+                  uint32_t *k_out, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s) {
     if (n1 == 0) {
         PSK_CUDA(cudaMemsetAsync(k_out, 0, sizeof(uint32_t), s));
         return PSACAK_OK;
@@ -299,16 +298,16 @@ status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t
     uint32_t grid = (uint32_t)(ceil_div(n1, 256) < (uint64_t)max_ctas * 4 ? ceil_div(n1, 256) : (uint64_t)max_ctas * 4);
     PSK_PROF_LAUNCH(s, "name_flags", n1, 0, (k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lms, sorted, n1, flags)));
     PSK_LAUNCH_CHECK();
-    return chunk_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags}, NameStore{sorted, lms, lms_pref, red, heads, n1},
-                                                 n1, partial, k_out, OpSum<uint32_t>(), max_ctas, s);
+    return lb_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags}, NameStore{sorted, lms, lms_pref, red, heads, n1}, n1,
+                                              k_out, OpSum<uint32_t>(), *env.ss, *env.os, env.err, s, "scan_names");
 }
 
 template status_t name_lms<uint8_t>(const uint8_t *, uint64_t, const uint32_t *, const uint32_t *, const uint32_t *,
-                                    uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t,
-                                    cudaStream_t);
+                                    uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *, const ScanEnv &,
+                                    uint32_t, cudaStream_t);
 template status_t name_lms<uint32_t>(const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
                                      const uint32_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *,
-                                     uint32_t *, uint32_t, cudaStream_t);
+                                     const ScanEnv &, uint32_t, cudaStream_t);
 
 __global__ void k_translate(uint32_t *red, uint64_t n1, const uint32_t *__restrict__ types,
                             const uint32_t *__restrict__ heads, uint32_t *err) {

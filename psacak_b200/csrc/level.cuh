@@ -3,7 +3,7 @@
 // bucket pointers, permutation of the reduced suffix array, tiny levels.
 #pragma once
 
-#include "prims.cuh"
+#include "lbscan.cuh"
 
 namespace psk {
 
@@ -12,6 +12,14 @@ constexpr int TYPE_BLOCK = 256;
 constexpr uint64_t TYPE_TILE = 32ull * TYPE_BLOCK;
 
 struct Workspace;  // fwd
+
+// What a single-pass scan needs: its flag/value scratch, the tickets and
+// launch epoch it shares with the onesweep kernels, and the error word.
+struct ScanEnv {
+    ScanScratch *ss;
+    OnesweepScratch *os;
+    uint32_t *err;
+};
 
 // Histograms of a byte level: per character its count, its L-type count and
 // its LMS count (the reference's Buckets::new, src/psacak8.rs:355-374).
@@ -24,15 +32,15 @@ struct ByteHist {
 // L/S typing of `text` into packed bitmaps: bit i of `types` is 1 iff
 // position i is S-type; bit i of `lms` is 1 iff position i is LMS.  Also
 // writes per-word LMS popcounts into `lms_wcnt` (nwords entries) and, for
-// bytes, accumulates `hist`.  `scratch` holds >= ntiles + 1024 uint32.
+// bytes, accumulates `hist`.  `scratch` holds >= 2 * ntiles uint32.
 template <class C>
 status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, uint32_t *lms_wcnt,
-                   ByteHist *hist, uint32_t *scratch, uint32_t max_ctas, cudaStream_t s);
+                   ByteHist *hist, uint32_t *scratch, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s);
 
 // Exclusive prefix of LMS popcounts: pref[w] = LMS positions before word w;
 // pref[nwords] = total, also copied to *total (device).
-status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *partial,
-                    uint32_t *total, uint32_t max_ctas, cudaStream_t s);
+status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *total,
+                    const ScanEnv &env, cudaStream_t s);
 
 // Rank of LMS position p among LMS positions (number of LMS before p).
 __device__ __forceinline__ uint32_t lms_rank(const uint32_t *lms, const uint32_t *pref, uint64_t p) {
@@ -48,7 +56,7 @@ __device__ __forceinline__ uint32_t lms_rank(const uint32_t *lms, const uint32_t
 template <class C>
 status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t *lms_pref,
                   const uint32_t *sorted, uint64_t n1, uint32_t *red, uint32_t *heads, uint32_t *flags,
-                  uint32_t *partial, uint32_t *k_out, uint32_t max_ctas, cudaStream_t s);
+                  uint32_t *k_out, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s);
 
 // Translates names in `red` (types in `types`) into bucket pointers in place:
 // L -> heads[c], S -> heads[c+1] - 1 (the reference's translate,
