@@ -499,9 +499,7 @@ void ctx_free(Ctx &c) {
     if (c.os.status) cudaFree(c.os.status);
     c.os.status = nullptr;
     if (c.ss.flags) cudaFree(c.ss.flags);
-    if (c.ss.vals) cudaFree(c.ss.vals);
     c.ss.flags = nullptr;
-    c.ss.vals = nullptr;
     c.ss.max_tiles = 0;
     c.os.tickets = nullptr;
     c.h_hist = nullptr;

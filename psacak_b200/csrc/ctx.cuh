@@ -158,14 +158,11 @@ struct Ctx {
         if (tiles <= ss.max_tiles) return PSACAK_OK;
         const uint64_t want = tiles + tiles / 4 + 64;
         if (ss.flags) cudaFreeAsync(ss.flags, stream);
-        if (ss.vals) cudaFreeAsync(ss.vals, stream);
         ss.flags = nullptr;
-        ss.vals = nullptr;
         ss.max_tiles = 0;
-        PSK_CUDA(cudaMallocAsync(&ss.flags, want * sizeof(uint64_t), stream));
-        PSK_CUDA(cudaMallocAsync(&ss.vals, want * 2 * LS_MAX_VALUE_BYTES, stream));
-        // zeroed flags read as "not ready" for every epoch
-        PSK_CUDA(cudaMemsetAsync(ss.flags, 0, want * sizeof(uint64_t), stream));
+        PSK_CUDA(cudaMallocAsync(&ss.flags, want * LS_MAX_FIELDS * sizeof(uint64_t), stream));
+        // zeroed words read as "not ready" for every epoch
+        PSK_CUDA(cudaMemsetAsync(ss.flags, 0, want * LS_MAX_FIELDS * sizeof(uint64_t), stream));
         ss.max_tiles = want;
         return PSACAK_OK;
     }
@@ -178,10 +175,13 @@ struct Ctx {
     }
     // Stable LSD radix sort of (key, value) pairs on bits [b0, b1); the
     // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).
+    // `hist_ready`: the digits were already counted into d_hist by the
+    // keys' producer.
     template <class K, class V>
-    status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1) {
+    status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1, bool hist_ready = false) {
         PSK_TRY(ensure_onesweep(ceil_div(n, 8 * OS_BLOCK) + 1));
-        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream, RADIX_IPT);
+        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream, RADIX_IPT,
+                                      hist_ready);
     }
     // Single-pass stable compaction (see compact1).
     template <class Pred, class Emit>

@@ -166,16 +166,53 @@ __global__ void k_init_cursors(const ByteGeom *__restrict__ g, const uint8_t *__
 }
 
 // ---- chain expansion -----------------------------------------------------
+//
+// The cells of a part (seed q, depth d = 1..runs[q]) go breadth-first: all
+// depth-1 cells in seed order, then depth 2, ...  The cell (q, d) therefore
+// lands at  first + C_1 + ... + C_{d-1} + #{q' < q : runs[q'] >= d},  where
+// C_d = #{q : runs[q] >= d}.  Depths 1..CHAIN_DIRECT are placed straight
+// from one scan over the seeds that counts, per seed, runs >= 1, >= 2, >= 3
+// and the cells deeper than that; only the deep cells (long runs of one
+// character, rare outside runs like N-blocks) go through a sort on depth.
+constexpr uint32_t CHAIN_DIRECT = 3;
+
+// Per-seed counters of the chain scan.
+struct ChainCounts {
+    uint32_t c1, c2, c3, deep;
+};
+__device__ __forceinline__ ChainCounts shfl_up_t(ChainCounts v, int o) {
+    ChainCounts r;
+    r.c1 = __shfl_up_sync(FULL_MASK, v.c1, o);
+    r.c2 = __shfl_up_sync(FULL_MASK, v.c2, o);
+    r.c3 = __shfl_up_sync(FULL_MASK, v.c3, o);
+    r.deep = __shfl_up_sync(FULL_MASK, v.deep, o);
+    return r;
+}
+struct OpChain {
+    static constexpr int kFields = 4;
+    __device__ __forceinline__ static uint32_t field(int, uint32_t a, uint32_t b) { return a + b; }
+    __device__ __forceinline__ ChainCounts operator()(ChainCounts a, ChainCounts b) const {
+        return ChainCounts{a.c1 + b.c1, a.c2 + b.c2, a.c3 + b.c3, a.deep + b.deep};
+    }
+    __device__ __forceinline__ static ChainCounts identity() { return ChainCounts{0, 0, 0, 0}; }
+};
+__device__ __forceinline__ ChainCounts chain_counts(uint32_t r) {
+    return ChainCounts{r >= 1 ? 1u : 0u, r >= 2 ? 1u : 0u, r >= 3 ? 1u : 0u, r > CHAIN_DIRECT ? r - CHAIN_DIRECT : 0u};
+}
 
 // Seeds in scan order: L part = sa[start + q]; S part = sa[start - q].
 // runs[q] = number of equal characters c in front of the seed; endc[q] =
 // the character in front of the run.  c0s[slot] (the character in front of
 // sa[slot]) was written beside every seed by whoever placed it, so the text
-// is only read inside runs.
-__global__ void k_seed_runs(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sa, uint32_t start, int dir,
-                            uint32_t nseeds, uint8_t c, uint32_t *runs, uint32_t *maxrun, const uint8_t *c0s,
-                            uint8_t *endc) {
+// is only read inside runs.  totals[0] = longest run (atomic max),
+// totals[1..4] = the part's ChainCounts (C_1, C_2, C_3, deep cells).
+__global__ void __launch_bounds__(256) k_seed_runs(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sa,
+                                                   uint32_t start, int dir, uint32_t nseeds, uint8_t c,
+                                                   uint32_t *runs, uint32_t *totals, const uint8_t *c0s,
+                                                   uint8_t *endc) {
+    __shared__ uint32_t s_red[8][5];
     uint32_t mx = 0;
+    ChainCounts acc{0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nseeds; q += gridDim.x * blockDim.x) {
         const uint32_t slot = dir > 0 ? start + q : start - q;
         uint32_t x = sa[slot];
@@ -192,42 +229,108 @@ __global__ void k_seed_runs(const uint8_t *__restrict__ text, const uint32_t *__
         endc[q] = before;
         runs[q] = r;
         mx = r > mx ? r : mx;
+        acc = OpChain()(acc, chain_counts(r));
     }
     for (int o = 16; o > 0; o >>= 1) {
         uint32_t t = __shfl_down_sync(FULL_MASK, mx, o);
         mx = t > mx ? t : mx;
+        acc.c1 += __shfl_down_sync(FULL_MASK, acc.c1, o);
+        acc.c2 += __shfl_down_sync(FULL_MASK, acc.c2, o);
+        acc.c3 += __shfl_down_sync(FULL_MASK, acc.c3, o);
+        acc.deep += __shfl_down_sync(FULL_MASK, acc.deep, o);
     }
-    if ((threadIdx.x & 31) == 0 && mx) atomicMax(maxrun, mx);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        s_red[w][0] = mx;
+        s_red[w][1] = acc.c1;
+        s_red[w][2] = acc.c2;
+        s_red[w][3] = acc.c3;
+        s_red[w][4] = acc.deep;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        uint32_t v = 0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) {
+            const uint32_t t = s_red[ww][threadIdx.x];
+            v = threadIdx.x == 0 ? (t > v ? t : v) : v + t;
+        }
+        if (v) {
+            if (threadIdx.x == 0) atomicMax(&totals[0], v);
+            else atomicAdd(&totals[threadIdx.x], v);
+        }
+    }
 }
 
-struct RunLoad {
-    const uint32_t *runs;
-    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return runs[i]; }
+// Chain scan: per seed its ChainCounts; the load also fetches the seed, its
+// run length and the character in front of its run, and the store writes
+// the seed's cells of depth 1..3 (entry and predecessor character) and the
+// offset of its deep cells.
+struct ChainPayload {
+    uint32_t x, r;
+    uint8_t e;
 };
-struct RunStore {
-    uint32_t *off;
-    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t) const { off[i] = excl; }
+struct ChainLoad {
+    using Payload = ChainPayload;
+    static constexpr int kIPT = 6;
+    const uint32_t *sa;
+    const uint32_t *runs;
+    const uint8_t *endc;
+    uint32_t start;
+    int dir;
+    __device__ __forceinline__ ChainCounts operator()(uint64_t q, ChainPayload &p) const {
+        p.x = sa[dir > 0 ? start + (uint32_t)q : start - (uint32_t)q];
+        p.r = runs[q];
+        p.e = endc[q];
+        return chain_counts(p.r);
+    }
+};
+struct ChainStore {
+    uint32_t *sa;
+    uint8_t *c0s;
+    uint32_t *deep_off;  // null when the part has no deep cells
+    uint32_t first;      // slot of the first cell
+    uint32_t base2, base3;  // C_1 and C_1 + C_2
+    uint32_t limit;         // cells of depth <= 3 (C_1 + C_2 + C_3)
+    int dir;
+    uint8_t c;
+    uint32_t *err;
+    __device__ __forceinline__ void put(uint32_t k, uint32_t val, uint8_t pc) const {
+        if (k >= limit) {
+            dev_fail(err, DEVERR_RANGE);
+            return;
+        }
+        const uint32_t slot = dir > 0 ? first + k : first - k;
+        sa[slot] = val;
+        c0s[slot] = pc;
+    }
+    __device__ __forceinline__ void operator()(uint64_t q, ChainCounts ex, ChainCounts, const ChainPayload &p) const {
+        const uint32_t r = p.r;
+        if (r >= 1) put(ex.c1, p.x - 1, r > 1 ? c : p.e);
+        if (r >= 2) put(base2 + ex.c2, p.x - 2, r > 2 ? c : p.e);
+        if (r >= 3) put(base3 + ex.c3, p.x - 3, r > 3 ? c : p.e);
+        if (deep_off) deep_off[q] = ex.deep;
+    }
 };
 
-// Cell q (row-major over seeds) -> (depth d, value (seed - d) << 8 | the
-// character in front of that suffix: c inside the run, the run's leading
-// character at its deepest member).
-__global__ void k_expand_cells(const uint32_t *__restrict__ sa, uint32_t start, int dir, uint32_t nseeds,
-                               const uint32_t *__restrict__ off, const uint32_t *__restrict__ runs,
-                               const uint8_t *__restrict__ endc, uint8_t c, uint32_t ncells, uint32_t *keys,
-                               uint64_t *vals) {
+// Deep cell q (row-major over seeds, depths > 3) -> (depth - 3, value
+// (seed - depth) << 8 | the character in front of that suffix).
+__global__ void k_expand_deep(const uint32_t *__restrict__ sa, uint32_t start, int dir, uint32_t nseeds,
+                              const uint32_t *__restrict__ off, const uint32_t *__restrict__ runs,
+                              const uint8_t *__restrict__ endc, uint8_t c, uint32_t ncells, uint32_t *keys,
+                              uint64_t *vals) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ncells; q += gridDim.x * blockDim.x) {
-        // last seed s with off[s] <= q
+        // last seed s with off[s] <= q (seeds without deep cells share the next one's offset)
         uint32_t lo = 0, hi = nseeds - 1;
         while (lo < hi) {
             uint32_t mid = (lo + hi + 1) >> 1;
             if (off[mid] <= q) lo = mid;
             else hi = mid - 1;
         }
-        uint32_t d = q - off[lo] + 1;
+        uint32_t dd = q - off[lo] + 1;
+        uint32_t d = dd + CHAIN_DIRECT;
         uint32_t x = sa[dir > 0 ? start + lo : start - lo];
         uint8_t pc = d < runs[lo] ? c : endc[lo];
-        keys[q] = d;
+        keys[q] = dd;
         vals[q] = ((uint64_t)(x - d) << 8) | pc;
     }
 }
@@ -335,29 +438,35 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     if (part == 0) return PSACAK_OK;
     if (nseeds == 0 || nseeds > part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds for a part of %u", c, nseeds, part);
-    uint32_t *d_max = ctx.d_scalars + 8;
-    uint32_t *d_tot = ctx.d_scalars + 9;
-    PSK_CUDA(cudaMemsetAsync(d_max, 0, sizeof(uint32_t), s));
+    uint32_t *d_tot = ctx.d_scalars + 24;  // [max run, C_1, C_2, C_3, deep cells]
+    PSK_CUDA(cudaMemsetAsync(d_tot, 0, 5 * sizeof(uint32_t), s));
     PSK_PROF_LAUNCH(s, "chain_runs", nseeds, 0,
-                    (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_max,
+                    (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_tot,
                                                                          c0s, endc)));
     if (nseeds == part) return PSACAK_OK;
-    PSK_TRY((ctx.scan<uint32_t, OpSum<uint32_t>>(RunLoad{runs}, RunStore{off}, nseeds, d_tot, OpSum<uint32_t>(),
-                                                 "scan_runs")));
-    uint32_t h[2];
-    PSK_TRY(ctx.read_u32(d_max, h, 2));
-    const uint32_t maxrun = h[0], ncells = h[1];
+    uint32_t h[5];
+    PSK_TRY(ctx.read_u32(d_tot, h, 5));
+    const uint32_t maxrun = h[0], C1 = h[1], C2 = h[2], C3 = h[3], ndeep = h[4];
+    const uint64_t ncells = (uint64_t)C1 + C2 + C3 + ndeep;
     if (nseeds + ncells != part)
-        return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds + %u chained != %u", c, nseeds, ncells, part);
-    PSK_PROF_LAUNCH(s, "chain_expand", ncells, 0,
-                    (k_expand_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, runs, endc, c,
-                                                                            ncells, k0, v0)));
+        return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds + %llu chained != %u", c, nseeds,
+                         (unsigned long long)ncells, part);
+    const uint32_t first = dir > 0 ? start + nseeds : start - nseeds;
+    const uint32_t direct = C1 + C2 + C3;
+    PSK_TRY((ctx.scan<ChainCounts, OpChain>(ChainLoad{sa, runs, endc, start, dir},
+                                            ChainStore{sa, c0s, ndeep ? off : nullptr, first, C1, C1 + C2, direct, dir,
+                                                       c, ctx.d_err},
+                                            nseeds, (ChainCounts *)nullptr, OpChain(), "chain_place")));
+    if (ndeep == 0) return PSACAK_OK;
+    PSK_PROF_LAUNCH(s, "chain_deep", ndeep, 0,
+                    (k_expand_deep<<<grid_cap(ndeep, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, runs, endc, c,
+                                                                           ndeep, k0, v0)));
     PSK_LAUNCH_CHECK();
     int in1 = 0;
-    PSK_TRY((ctx.radix_sort<uint32_t, uint64_t>(k0, v0, k1, v1, ncells, 0, bitlen(maxrun), &in1)));
-    uint32_t first = dir > 0 ? start + nseeds : start - nseeds;
-    PSK_PROF_LAUNCH(s, "chain_place", ncells, 13ull * ncells,
-                    (k_place_cells<<<grid_cap(ncells, 8192), 256, 0, s>>>(in1 ? v1 : v0, ncells, first, dir, sa, c0s)));
+    PSK_TRY((ctx.radix_sort<uint32_t, uint64_t>(k0, v0, k1, v1, ndeep, 0, bitlen(maxrun - CHAIN_DIRECT), &in1)));
+    const uint32_t dfirst = dir > 0 ? first + direct : first - direct;
+    PSK_PROF_LAUNCH(s, "chain_place_deep", ndeep, 13ull * ndeep,
+                    (k_place_cells<<<grid_cap(ndeep, 8192), 256, 0, s>>>(in1 ? v1 : v0, ndeep, dfirst, dir, sa, c0s)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }

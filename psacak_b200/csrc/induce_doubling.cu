@@ -41,6 +41,10 @@ __device__ __forceinline__ Tri shfl_up_t(Tri v, int o) {
     return r;
 }
 struct OpTri {
+    static constexpr int kFields = 4;  // g, s: max; k, o: sum
+    __device__ __forceinline__ static uint32_t field(int f, uint32_t a, uint32_t b) {
+        return f < 2 ? (a > b ? a : b) : a + b;
+    }
     __device__ __forceinline__ Tri operator()(Tri a, Tri b) const {
         Tri r;
         r.g = a.g > b.g ? a.g : b.g;
@@ -93,28 +97,33 @@ __global__ void k_place_lms_any(const C *__restrict__ text, uint64_t nwords, con
 // src/psacak32.rs:103-121).  `last` = index of the last list entry of the
 // same bucket, found by a max-scan over the reversed list.
 template <class C> struct LastLoad {
+    static constexpr int kIPT = 8;
+    struct Payload {
+        uint32_t p;     // the LMS position
+        uint32_t tail;  // tail slot (+1) of its bucket
+    };
     const C *text;
     const uint32_t *sorted;
     uint64_t n1;
     Geom<C> g;
-    __device__ __forceinline__ uint32_t operator()(uint64_t r) const {
+    __device__ __forceinline__ uint32_t operator()(uint64_t r, Payload &pl) const {
         uint64_t i = n1 - 1 - r;
-        bool last = (i + 1 == n1) || g.bucket(text[sorted[i + 1]]) != g.bucket(text[sorted[i]]);
+        pl.p = sorted[i];
+        const C c = text[pl.p];
+        pl.tail = g.tail(c);
+        bool last = (i + 1 == n1) || g.bucket(text[sorted[i + 1]]) != g.bucket(c);
         return last ? (uint32_t)(r + 1) : 0u;
     }
 };
 template <class C> struct LastStore {
-    const C *text;
-    const uint32_t *sorted;
     uint64_t n1;
-    Geom<C> g;
     uint32_t *R;
-    __device__ __forceinline__ void operator()(uint64_t r, uint32_t excl, uint32_t v) const {
+    __device__ __forceinline__ void operator()(uint64_t r, uint32_t excl, uint32_t v,
+                                               const typename LastLoad<C>::Payload &pl) const {
         uint32_t inc = excl > v ? excl : v;
         uint64_t i = n1 - 1 - r;
         uint64_t last = n1 - inc;
-        uint32_t p = sorted[i];
-        R[p] = g.tail(text[p]) - (uint32_t)(last - i);
+        R[pl.p] = pl.tail - (uint32_t)(last - i);
     }
 };
 
@@ -165,26 +174,60 @@ __global__ void k_group_starts(Geom<C> g, uint64_t nbuckets, uint32_t *gstart) {
         gstart[c] = STYPE ? g.sstart_of((uint32_t)c) : g.lstart_of((uint32_t)c);
 }
 
-__global__ void k_keys(const uint32_t *__restrict__ Wg, const uint32_t *__restrict__ Wv, uint64_t cnt,
-                       const uint32_t *__restrict__ R, uint64_t n, uint64_t h, int KB, uint64_t *keys,
-                       uint32_t *vals, uint32_t *err) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t v = Wv[i];
-        uint64_t q = (uint64_t)v + h;
-        uint32_t r = 0;
-        if (q <= n) r = R[q];
-        else dev_fail(err, DEVERR_RANGE);
-        keys[i] = ((uint64_t)Wg[i] << KB) | r;
-        vals[i] = v;
+// Keys of one round: (group id, rank of j + h).  The block also counts the
+// digits of every radix pass of the keys (bits [0, nbits)) into `hist`, so
+// the sort needs no histogram pass of its own.
+__global__ void __launch_bounds__(256) k_keys(const uint32_t *__restrict__ Wg, const uint32_t *__restrict__ Wv,
+                                              uint64_t cnt, const uint32_t *__restrict__ R, uint64_t n, uint64_t h,
+                                              int KB, uint64_t *keys, uint32_t *vals, int nbits, uint32_t *hist,
+                                              uint32_t *err) {
+    __shared__ uint32_t sh[RADIX_MAX_PASSES * 256];
+    const int npasses = (nbits + 7) / 8;
+    for (int i = threadIdx.x; i < npasses * 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t ib = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); ib < cnt; ib += stride) {
+        const uint64_t i = ib + (threadIdx.x & 31);
+        const bool valid = i < cnt;
+        uint64_t key = 0;
+        if (valid) {
+            const uint32_t v = Wv[i];
+            const uint64_t q = (uint64_t)v + h;
+            uint32_t r = 0;
+            if (q <= n) r = R[q];
+            else dev_fail(err, DEVERR_RANGE);
+            key = ((uint64_t)Wg[i] << KB) | r;
+            keys[i] = key;
+            vals[i] = v;
+        }
+        radix_count_digits(sh, key, valid, 0, npasses, nbits);
     }
+    __syncthreads();
+    radix_flush_digits(sh, npasses, hist);
 }
 
+// The load also fetches the item's position and its group's first slot
+// (the store's only reads), so their latency overlaps the scan.
+struct RoundPayload {
+    uint32_t val;  // position
+    uint32_t gs;   // first slot of the item's group
+};
 struct RoundLoad {
+    using Payload = RoundPayload;
+    static constexpr int kIPT = 6;
     const uint64_t *keys;
-    uint64_t cnt;
+    const uint32_t *vals;
+    const uint32_t *gstart;  // group id -> first slot (this round)
+    uint64_t cnt, n, ngroups;
     int KB;
-    __device__ __forceinline__ Tri operator()(uint64_t i) const {
+    uint32_t *err;
+    __device__ __forceinline__ Tri operator()(uint64_t i, RoundPayload &pl) const {
         uint64_t k = keys[i];
+        const uint64_t gid = k >> KB;
+        pl.val = vals[i];
+        pl.gs = 0;
+        if (gid < ngroups && pl.val < n) pl.gs = gstart[gid];
+        else pl.val = 0xFFFFFFFFu;  // reported by the store
         bool gb = true, sb = true, sbn = true;
         if (i > 0) {
             uint64_t kp = keys[i - 1];
@@ -202,24 +245,19 @@ struct RoundLoad {
     }
 };
 struct RoundStore {
-    const uint64_t *keys;
-    const uint32_t *vals;
-    int KB;
-    const uint32_t *gstart;  // group id -> first slot (this round)
-    uint32_t *gnext;         // kept subgroup ordinal -> first slot (next round)
+    uint32_t *gnext;  // kept subgroup ordinal -> first slot (next round)
     uint32_t *R, *sa, *Wg, *Wv;
-    uint64_t n, ngroups;
+    uint64_t n;
     uint32_t *err;
-    __device__ __forceinline__ void operator()(uint64_t i, Tri excl, Tri v) const {
+    __device__ __forceinline__ void operator()(uint64_t i, Tri excl, Tri v, const RoundPayload &pl) const {
         uint32_t gs = (excl.g > v.g ? excl.g : v.g) - 1;
         uint32_t ss = (excl.s > v.s ? excl.s : v.s) - 1;
-        uint64_t gid = keys[i] >> KB;
-        uint32_t val = vals[i];
-        if (gid >= ngroups || val >= n) {
+        const uint32_t val = pl.val;
+        if (val >= n) {
             dev_fail(err, DEVERR_RANGE);
             return;
         }
-        uint32_t newg = gstart[gid] + (ss - gs);
+        uint32_t newg = pl.gs + (ss - gs);
         if (newg >= n) {
             dev_fail(err, DEVERR_RANGE);
             return;
@@ -269,18 +307,19 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
     for (uint64_t h = 1; cnt > 0; h <<= 1) {
         const int GB = bitlen(ngroups > 0 ? ngroups - 1 : 0);
         if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
-        uint64_t gblocks = ceil_div(cnt, 256);
+        uint64_t gblocks = ceil_div(cnt, 256 * 16);
+        PSK_CUDA(cudaMemsetAsync(ctx.d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
         PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
-                        (k_keys<<<(uint32_t)(gblocks < 16384 ? gblocks : 16384), 256, 0, s>>>(Wg, Wv, cnt, R, n, h, KB,
-                                                                                              k0, v0, ctx.d_err)));
+                        (k_keys<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
+                            Wg, Wv, cnt, R, n, h, KB, k0, v0, KB + GB, ctx.d_hist, ctx.d_err)));
         PSK_LAUNCH_CHECK();
         int in1 = 0;
-        PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, &in1)));
+        PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, &in1, true)));
         const uint64_t *ks = in1 ? k1 : k0;
         const uint32_t *vs = in1 ? v1 : v0;
-        PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, cnt, KB},
-                                      RoundStore{ks, vs, KB, gA, gB, R, sa, Wg, Wv, n, ngroups, ctx.d_err}, cnt, d_tri,
-                                      OpTri(), "scan_rounds")));
+        PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, ngroups, KB, ctx.d_err},
+                                      RoundStore{gB, R, sa, Wg, Wv, n, ctx.d_err}, cnt, d_tri, OpTri(),
+                                      "scan_rounds")));
         uint32_t tri[4];
         PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
         if (ctx.stage_timing)
@@ -320,7 +359,7 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
         PSK_LAUNCH_CHECK();
     } else if (n1 > 0) {
         PSK_TRY((ctx.scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{text, sorted_lms, n1, geom},
-                                                     LastStore<C>{text, sorted_lms, n1, geom, R}, n1,
+                                                     LastStore<C>{n1, R}, n1,
                                                      (uint32_t *)nullptr, OpMax<uint32_t>(), "scan_last")));
     }
     PSK_TRY((doubling_scan<C, false>(ctx, text, n, types, geom, nbuckets, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, s)));

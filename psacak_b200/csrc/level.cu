@@ -268,20 +268,27 @@ __global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint3
     }
 }
 
+// The load also finds the text-order rank of the LMS position (two gathers),
+// so that the store only writes.
 struct NameLoad {
+    using Payload = uint32_t;  // rank of sorted[i] among the LMS positions
+    static constexpr int kIPT = 8;
     const uint32_t *flags;
-    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return flags[i]; }
-};
-struct NameStore {
     const uint32_t *sorted;
     const uint32_t *lms;
     const uint32_t *pref;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i, uint32_t &rank) const {
+        rank = lms_rank(lms, pref, sorted[i]);
+        return flags[i];
+    }
+};
+struct NameStore {
     uint32_t *red;
     uint32_t *heads;
     uint64_t n1;
-    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t v) const {
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t excl, uint32_t v, uint32_t rank) const {
         uint32_t name = excl + v - 1;
-        red[lms_rank(lms, pref, sorted[i])] = name;
+        red[rank] = name;
         if (v) heads[name] = (uint32_t)i;
         if (i == n1 - 1) heads[name + 1] = (uint32_t)n1;
     }
@@ -298,7 +305,7 @@ status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t
     uint32_t grid = (uint32_t)(ceil_div(n1, 256) < (uint64_t)max_ctas * 4 ? ceil_div(n1, 256) : (uint64_t)max_ctas * 4);
     PSK_PROF_LAUNCH(s, "name_flags", n1, 0, (k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lms, sorted, n1, flags)));
     PSK_LAUNCH_CHECK();
-    return lb_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags}, NameStore{sorted, lms, lms_pref, red, heads, n1}, n1,
+    return lb_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags, sorted, lms, lms_pref}, NameStore{red, heads, n1}, n1,
                                               k_out, OpSum<uint32_t>(), *env.ss, *env.os, env.err, s, "scan_names");
 }
 

@@ -18,13 +18,20 @@ namespace psk {
 
 constexpr uint32_t MAX_CHUNKS = 1024;  // cap on the CTAs of grid-stride helper kernels
 
+// Scan operators.  kFields / field(f, a, b): the value as 32-bit fields and
+// the combination of field f (the single-pass scan publishes each field on
+// its own).
 template <class T> struct OpSum {
+    static constexpr int kFields = 1;
     __device__ __forceinline__ T operator()(T a, T b) const { return a + b; }
     __device__ __forceinline__ static T identity() { return T(0); }
+    __device__ __forceinline__ static uint32_t field(int, uint32_t a, uint32_t b) { return a + b; }
 };
 template <class T> struct OpMax {
+    static constexpr int kFields = 1;
     __device__ __forceinline__ T operator()(T a, T b) const { return a > b ? a : b; }
     __device__ __forceinline__ static T identity() { return T(0); }
+    __device__ __forceinline__ static uint32_t field(int, uint32_t a, uint32_t b) { return a > b ? a : b; }
 };
 
 // Shuffle-up of any scan value; aggregate value types provide an overload

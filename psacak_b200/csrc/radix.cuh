@@ -205,23 +205,54 @@ __global__ void __launch_bounds__(RADIX_HIST_BLOCK) k_radix_hist(const K *__rest
         if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
+// Digit counting for kernels that produce radix keys: each thread of a
+// block adds its key (valid or not: every lane of the warp must call it) to
+// the block's shared histograms sh[p * 256 + d]; radix_flush_digits adds
+// them to the device histograms at the end of the block.
+template <class K>
+__device__ __forceinline__ void radix_count_digits(uint32_t *sh, K k, bool valid, int begin_bit, int npasses,
+                                                   int end_bit) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t vmask = __ballot_sync(FULL_MASK, valid);
+    for (int p = 0; p < npasses; p++) {
+        int shift = begin_bit + 8 * p;
+        int bits = end_bit - shift < 8 ? end_bit - shift : 8;
+        uint32_t d = (uint32_t)(k >> shift) & ((1u << bits) - 1);
+        uint32_t d0 = __shfl_sync(FULL_MASK, d, 0);
+        if (__all_sync(FULL_MASK, !valid || d == d0)) {
+            if (lane == 0 && vmask) atomicAdd(&sh[p * 256 + d0], __popc(vmask));
+        } else if (valid) {
+            atomicAdd(&sh[p * 256 + d], 1u);
+        }
+    }
+}
+__device__ __forceinline__ void radix_flush_digits(const uint32_t *sh, int npasses, uint32_t *hist) {
+    for (int i = threadIdx.x; i < npasses * 256; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
 // Exclusive digit bases per pass (one block of 256 threads per pass).
 __global__ void k_radix_bases(const uint32_t *hist, uint32_t *bases);
 
+// When `hist_ready` is set, the producer of the keys has already counted
+// the digits of every pass into d_hist (see radix_count_digits), and the
+// histogram kernel is skipped.
 template <class K, class V>
 status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit, int end_bit, uint32_t *d_hist,
                           uint32_t *h_hist, OnesweepScratch &sc, uint32_t *err, int *result_in_1, cudaStream_t s,
-                          int ipt = 12) {
+                          int ipt = 12, bool hist_ready = false) {
     *result_in_1 = 0;
     if (n <= 1 || end_bit <= begin_bit) return PSACAK_OK;
     const int npasses = (end_bit - begin_bit + 7) / 8;
     if (npasses > RADIX_MAX_PASSES) return set_error(PSACAK_EINTERNAL, "radix sort: too many passes");
     uint32_t *bases = d_hist + RADIX_MAX_PASSES * 256;
-    PSK_CUDA(cudaMemsetAsync(d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
-    uint64_t g = ceil_div(n, RADIX_HIST_BLOCK * 16);
-    PSK_PROF_LAUNCH(s, "radix_hist", n, n * sizeof(K),
-                    (k_radix_hist<K><<<(uint32_t)(g < 1184 ? g : 1184), RADIX_HIST_BLOCK, 0, s>>>(
-                        k0, n, begin_bit, npasses, end_bit, d_hist)));
+    if (!hist_ready) {
+        PSK_CUDA(cudaMemsetAsync(d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
+        uint64_t g = ceil_div(n, RADIX_HIST_BLOCK * 16);
+        PSK_PROF_LAUNCH(s, "radix_hist", n, n * sizeof(K),
+                        (k_radix_hist<K><<<(uint32_t)(g < 1184 ? g : 1184), RADIX_HIST_BLOCK, 0, s>>>(
+                            k0, n, begin_bit, npasses, end_bit, d_hist)));
+    }
     PSK_PROF_LAUNCH(s, "radix_bases", npasses * 256, 0, (k_radix_bases<<<npasses, 256, 0, s>>>(d_hist, bases)));
     PSK_CUDA(cudaMemcpyAsync(h_hist, d_hist, npasses * 256 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     PSK_CUDA(cudaStreamSynchronize(s));
