@@ -211,25 +211,46 @@ __global__ void __launch_bounds__(256) k_seed_runs(const uint8_t *__restrict__ t
                                                    uint32_t *runs, uint32_t *totals, const uint8_t *c0s,
                                                    uint8_t *endc) {
     __shared__ uint32_t s_red[8][5];
+    constexpr int U = 4;  // seeds per thread step: their loads and first gathers overlap
     uint32_t mx = 0;
     ChainCounts acc{0, 0, 0, 0};
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nseeds; q += gridDim.x * blockDim.x) {
-        const uint32_t slot = dir > 0 ? start + q : start - q;
-        uint32_t x = sa[slot];
-        uint32_t r = 0;
-        uint8_t before = 0;
-        if (x > 0) {
-            before = c0s[slot];
-            if (before == c) {
-                r = 1;
-                while (r < x && (before = text[x - r - 1]) == c) r++;
-                if (r == x) before = 0;
-            }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint64_t q0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q0 < nseeds; q0 += (uint64_t)stride * U) {
+        uint32_t x[U], slot[U];
+        uint8_t before[U], nxt[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t q = q0 + (uint64_t)u * stride;
+            slot[u] = dir > 0 ? start + (uint32_t)q : start - (uint32_t)q;
+            x[u] = q < nseeds ? sa[slot[u]] : 0u;
         }
-        endc[q] = before;
-        runs[q] = r;
-        mx = r > mx ? r : mx;
-        acc = OpChain()(acc, chain_counts(r));
+#pragma unroll
+        for (int u = 0; u < U; u++) before[u] = x[u] > 0 ? c0s[slot[u]] : 0;
+#pragma unroll
+        for (int u = 0; u < U; u++) nxt[u] = (before[u] == c && x[u] >= 2) ? text[x[u] - 2] : 0;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t q = q0 + (uint64_t)u * stride;
+            if (q >= nseeds) continue;
+            uint32_t r = 0;
+            uint8_t b = before[u];
+            if (x[u] > 0 && b == c) {
+                // the run holds x-1; nxt = text[x-2] is already here
+                r = 1;
+                if (r < x[u]) {
+                    b = nxt[u];
+                    if (b == c) {
+                        r = 2;
+                        while (r < x[u] && (b = text[x[u] - r - 1]) == c) r++;
+                    }
+                }
+                if (r == x[u]) b = 0;
+            }
+            endc[q] = b;
+            runs[q] = r;
+            mx = r > mx ? r : mx;
+            acc = OpChain()(acc, chain_counts(r));
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         uint32_t t = __shfl_down_sync(FULL_MASK, mx, o);

@@ -129,10 +129,37 @@ template <class C> struct LastStore {
 
 // ---- work list -----------------------------------------------------------
 
-template <class C, bool STYPE> struct WPred {
+// The work list is a stable compaction of the positions of one type: a scan
+// over the 32-position type words' popcounts gives every word its first
+// slot, then a kernel with a thread per position emits the selected ones
+// (slot = word's first slot + selected positions before it in the word).
+template <bool STYPE> __device__ __forceinline__ uint32_t selected_bits(const uint32_t *types, uint64_t n, uint64_t w) {
+    uint32_t bits = STYPE ? types[w] : ~types[w];
+    const uint64_t p0 = w << 5;
+    if (n - p0 < 32) bits &= (1u << (uint32_t)(n - p0)) - 1u;
+    return bits;
+}
+template <bool STYPE> struct WordLoad {
     const uint32_t *types;
-    __device__ __forceinline__ bool operator()(uint64_t j) const { return bm_get(types, j) == STYPE; }
+    uint64_t n;
+    __device__ __forceinline__ uint32_t operator()(uint64_t w) const { return __popc(selected_bits<STYPE>(types, n, w)); }
 };
+struct WordStore {
+    uint32_t *first;
+    __device__ __forceinline__ void operator()(uint64_t w, uint32_t excl, uint32_t) const { first[w] = excl; }
+};
+template <bool STYPE, class Emit>
+__global__ void k_emit_selected(const uint32_t *__restrict__ types, const uint32_t *__restrict__ first, uint64_t n,
+                                Emit emit) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: lanes stay word-aligned
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const uint64_t w = j >> 5;
+        const uint32_t bits = selected_bits<STYPE>(types, n, w);
+        if ((bits >> lane) & 1u) emit(j, first[w] + __popc(bits & ((1u << lane) - 1u)));
+    }
+}
+
 // Work item = (dense group id, position); the group id of round 1 is the
 // symbol's name and gstart[id] the first SA slot of its L (or S) part.
 template <class C, bool STYPE> struct WEmit {
@@ -290,7 +317,18 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
         PSK_KCOUNT();
         PSK_LAUNCH_CHECK();
     }
-    PSK_TRY(ctx.compact(WPred<C, STYPE>{types}, WEmit<C, STYPE>{text, geom, Wg, Wv, R}, n, d_cnt, "double_items"));
+    {
+        const uint64_t nwords = ceil_div(n, 32);
+        DBuf<uint32_t> first;
+        PSK_TRY(first.init(ctx, nwords));
+        PSK_TRY((ctx.scan<uint32_t, OpSum<uint32_t>>(WordLoad<STYPE>{types, n}, WordStore{first}, nwords, d_cnt,
+                                                     OpSum<uint32_t>(), "double_words")));
+        const uint64_t g = ceil_div(n, 256);
+        PSK_PROF_LAUNCH(s, "double_items", n, 0,
+                        (k_emit_selected<STYPE, WEmit<C, STYPE>><<<(uint32_t)(g < 16384 ? g : 16384), 256, 0, s>>>(
+                            types, first, n, WEmit<C, STYPE>{text, geom, Wg, Wv, R})));
+        PSK_LAUNCH_CHECK();
+    }
     uint32_t cnt = 0;
     PSK_TRY(ctx.read_u32(d_cnt, &cnt));
     return doubling_rounds(ctx, n, nbuckets, cnt, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, STYPE ? 'S' : 'L', s);
