@@ -247,24 +247,74 @@ __device__ __forceinline__ uint64_t next_lms(const uint32_t *lms, uint64_t n, ui
     return (w << 5) + (uint64_t)(__ffs(word) - 1);
 }
 
+// Fingerprint of the LMS substring at p: its length up to the next LMS
+// position (or "reaches the end", which equals nothing) and its first 16
+// bytes packed, zero-padded -- the GPU form of UintFingerprint::get
+// (src/naming.rs:339-385).  Equal fingerprints decide equality outright
+// when the substring fits in them; longer ones compare their remaining
+// characters.
+template <class C> struct LmsFp {
+    static constexpr uint32_t W = 16 / sizeof(C);  // characters held
+    static constexpr uint32_t END = 0xFFFFFFFFu;
+    uint32_t len;   // next LMS - p, or END
+    uint32_t w[4];  // first min(len + 1, W) characters
+};
 template <class C>
-__device__ bool lms_equal(const C *text, uint64_t n, const uint32_t *lms, uint64_t a, uint64_t b) {
-    uint64_t ea = next_lms(lms, n, a), eb = next_lms(lms, n, b);
-    if (ea >= n || eb >= n) return false;
-    uint64_t la = ea - a, lb = eb - b;
-    if (la != lb) return false;
-    for (uint64_t k = 0; k <= la; k++)
+__device__ __forceinline__ LmsFp<C> lms_fp(const C *text, uint64_t n, const uint32_t *lms, uint64_t p) {
+    LmsFp<C> f;
+    const uint64_t e = next_lms(lms, n, p);
+    f.len = e >= n ? LmsFp<C>::END : (uint32_t)(e - p);
+#pragma unroll
+    for (int i = 0; i < 4; i++) f.w[i] = 0;
+    const uint32_t take = f.len == LmsFp<C>::END ? 0u : (f.len + 1 < LmsFp<C>::W ? f.len + 1 : LmsFp<C>::W);
+    for (uint32_t k = 0; k < take; k++) {
+        const uint32_t c = (uint32_t)text[p + k];
+        if (sizeof(C) == 1) f.w[k >> 2] |= c << ((k & 3) * 8);
+        else f.w[k] = c;
+    }
+    return f;
+}
+template <class C>
+__device__ __forceinline__ bool lms_fp_equal(const C *text, const LmsFp<C> &fa, uint64_t a, const LmsFp<C> &fb,
+                                             uint64_t b) {
+    if (fa.len == LmsFp<C>::END || fa.len != fb.len) return false;
+    if (fa.w[0] != fb.w[0] || fa.w[1] != fb.w[1] || fa.w[2] != fb.w[2] || fa.w[3] != fb.w[3]) return false;
+    for (uint64_t k = LmsFp<C>::W; k <= fa.len; k++)
         if (text[a + k] != text[b + k]) return false;
     return true;
 }
 
+// flags[i] = 1 iff sorted LMS substring i differs from i - 1.  Each thread
+// fingerprints its own substring once and takes its neighbour's from the
+// lane below (lane 0 fingerprints its neighbour itself).
 template <class C>
 __global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint32_t *__restrict__ lms,
                              const uint32_t *__restrict__ sorted, uint64_t n1, uint32_t *flags) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t f = 1;
-        if (i > 0) f = lms_equal(text, n, lms, sorted[i - 1], sorted[i]) ? 0u : 1u;
-        flags[i] = f;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32
+    for (uint64_t ib = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); ib < n1; ib += stride) {
+        const uint64_t i = ib + lane;
+        const bool valid = i < n1;
+        const uint64_t p = valid ? sorted[i] : 0;
+        LmsFp<C> f;
+        if (valid) f = lms_fp(text, n, lms, p);
+        else f.len = LmsFp<C>::END;
+        uint64_t q = __shfl_up_sync(FULL_MASK, p, 1);
+        LmsFp<C> g;
+        g.len = __shfl_up_sync(FULL_MASK, f.len, 1);
+#pragma unroll
+        for (int k = 0; k < 4; k++) g.w[k] = __shfl_up_sync(FULL_MASK, f.w[k], 1);
+        if (valid) {
+            uint32_t flag = 1;
+            if (i > 0) {
+                if (lane == 0) {
+                    q = sorted[i - 1];
+                    g = lms_fp(text, n, lms, q);
+                }
+                flag = lms_fp_equal(text, g, q, f, p) ? 0u : 1u;
+            }
+            flags[i] = flag;
+        }
     }
 }
 
