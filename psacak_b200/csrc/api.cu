@@ -233,6 +233,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
 
     // Stage 2: name them and build the reduced string.
     DBuf<uint32_t> red, heads, flags, sa1, names1;
+    DBuf<uint64_t> sorted_pc;  // byte levels, bucket engine: final-mode LMS list with predecessor characters
     uint32_t k = 0;
     if (n1 > 0 && !extracted) {
         PSK_TRY(ctx.compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_scalars + 1,
@@ -298,8 +299,19 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
             trace_push(ctx, level, width, n, n1, k, 0);
             PSK_TRY(direct_inverse(red, n1, sa1, ctx.d_err, s));
         }
+        if constexpr (sizeof(C) == 1) {
+            if (engine == PSACAK_ENGINE_BUCKET) {
+                // the bucket scans take the list with predecessor characters
+                red.reset();
+                names1.reset();
+                DBuf<uint64_t> plist;
+                PSK_TRY(sorted_pc.init(ctx, n1));
+                PSK_TRY(plist.init(ctx, n1));
+                PSK_TRY(permute_lms8(sa1, n1, text, lms, pref, n, plist, sorted_pc, ctx.d_err, s));
+            }
+        }
         // red is free again; reuse it as the position list of the permutation.
-        PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
+        if (!sorted_pc.get()) PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
     } else {
         if (level == 0 && ctx.debug_red) {
             ctx.debug_n1 = 0;
@@ -314,8 +326,10 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
 
     // Stage 3: induce the whole suffix array from the sorted LMS suffixes.
     if constexpr (sizeof(C) == 1) {
-        if (engine == PSACAK_ENGINE_BUCKET)
-            return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sa1, n1, sa, s);
+        if (engine == PSACAK_ENGINE_BUCKET) {
+            sa1.reset();
+            return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sorted_pc, n1, sa, s);
+        }
         return induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
     } else {
         return induce_doubling<C>(ctx, text, n, types, lms, geom, nbuckets, INDUCE_FINAL, sa1, n1, nullptr, sa, s);

@@ -115,39 +115,26 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
 }
 
 // Final mode placement: the sorted LMS suffixes fill the tail of each
-// bucket in order.  Four entries per thread step so their text gathers
-// overlap; the bucket geometry is read from shared memory.
-constexpr int PS_UNROLL = 4;
-__global__ void __launch_bounds__(256) k_place_lms_sorted8(const uint8_t *__restrict__ text,
-                                                           const uint32_t *__restrict__ sorted, uint64_t n1,
+// bucket in order.  Entry i of the list is (position << 8 | predecessor
+// character); its bucket is the one whose LMS range holds i (a binary
+// search over the 256 ranges in shared memory), so the text is not read.
+__global__ void __launch_bounds__(256) k_place_lms_sorted8(const uint64_t *__restrict__ sorted, uint64_t n1,
                                                            const ByteGeom *__restrict__ g, uint32_t *sa,
                                                            uint8_t *c0s) {
-    __shared__ uint32_t s_off[256];  // slot of list entry i = s_off[c] + i
+    __shared__ uint32_t s_start[256], s_off[256];  // slot of list entry i = s_off[c] + i
+    s_start[threadIdx.x] = g->lmsstart[threadIdx.x];
     s_off[threadIdx.x] = g->tail[threadIdx.x] - g->lmscount[threadIdx.x] - g->lmsstart[threadIdx.x];
     __syncthreads();
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n1; i0 += stride * PS_UNROLL) {
-        uint32_t p[PS_UNROLL];
-        uint8_t c[PS_UNROLL], pc[PS_UNROLL];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = sorted[i];
+        // largest c with s_start[c] <= i (empty buckets share the next start)
+        uint32_t c = 0;
 #pragma unroll
-        for (int u = 0; u < PS_UNROLL; u++) {
-            const uint64_t i = i0 + (uint64_t)u * stride;
-            p[u] = i < n1 ? sorted[i] : 1u;
-        }
-#pragma unroll
-        for (int u = 0; u < PS_UNROLL; u++) {
-            c[u] = text[p[u]];
-            pc[u] = text[p[u] - 1];  // LMS positions are > 0
-        }
-#pragma unroll
-        for (int u = 0; u < PS_UNROLL; u++) {
-            const uint64_t i = i0 + (uint64_t)u * stride;
-            if (i < n1) {
-                const uint32_t slot = s_off[c[u]] + (uint32_t)i;
-                sa[slot] = p[u];
-                c0s[slot] = pc[u];
-            }
-        }
+        for (uint32_t step = 128; step > 0; step >>= 1)
+            if (s_start[c + step] <= (uint32_t)i) c += step;
+        const uint32_t slot = s_off[c] + (uint32_t)i;
+        sa[slot] = (uint32_t)(v >> 8);
+        c0s[slot] = (uint8_t)v;
     }
 }
 
@@ -514,7 +501,7 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
 }
 
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms, const ByteGeom &hg,
-                        const ByteGeom *dgeom, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
+                        const ByteGeom *dgeom, InduceMode mode, const uint64_t *sorted_pc, uint64_t n1,
                         uint32_t *sa, cudaStream_t s, uint32_t *lms_out) {
     uint32_t maxpart = 1, maxbucket = 1;
     for (int c = 0; c < 256; c++) {
@@ -550,7 +537,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
                                                                          wchunk)));
     } else if (n1 > 0) {
         PSK_PROF_LAUNCH(s, "place_lms", n1, 0,
-                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(text, sorted_lms, n1, dgeom, sa,
+                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(sorted_pc, n1, dgeom, sa,
                                                                                   c0s.get())));
     }
     k_init_cursors<<<1, 256, 0, s>>>(dgeom, text, n, curL, curS, sa, c0s.get());

@@ -289,7 +289,9 @@ struct RoundStore {
             dev_fail(err, DEVERR_RANGE);
             return;
         }
-        R[val] = newg + 1;
+        // Every item's rank is its group's first slot + 1 when the round
+        // starts; items of the group's first subgroup keep it.
+        if (ss != gs) R[val] = newg + 1;
         if (v.k) {
             uint32_t ord = excl.o + v.o - 1;
             Wg[excl.k] = ord;

@@ -429,6 +429,51 @@ status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint
     return PSACAK_OK;
 }
 
+// Byte levels: the permuted list carries each LMS position's predecessor
+// character, (p << 8) | text[p - 1], so that the final placement needs no
+// gather from the text.
+__global__ void k_lms_list8(const uint8_t *__restrict__ text, const uint32_t *__restrict__ lms,
+                            const uint32_t *__restrict__ pref, uint64_t nwords, uint64_t *plist) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t word = lms[w];
+        uint32_t o = pref[w];
+        while (word) {
+            int b = __ffs(word) - 1;
+            const uint64_t p = (w << 5) + b;  // LMS positions are > 0
+            plist[o++] = (p << 8) | text[p - 1];
+            word &= word - 1;
+        }
+    }
+}
+
+__global__ void k_permute8(const uint32_t *__restrict__ sa1, uint64_t n1, const uint64_t *__restrict__ plist,
+                           uint64_t *out, uint32_t *err) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t r = sa1[i];
+        if (r >= n1) {
+            dev_fail(err, DEVERR_RANGE);
+            out[i] = 1ull << 8;
+            continue;
+        }
+        out[i] = plist[r];
+    }
+}
+
+status_t permute_lms8(const uint32_t *sa1, uint64_t n1, const uint8_t *text, const uint32_t *lms,
+                      const uint32_t *lms_pref, uint64_t n, uint64_t *plist, uint64_t *out, uint32_t *err,
+                      cudaStream_t s) {
+    if (n1 == 0) return PSACAK_OK;
+    uint64_t nwords = ceil_div(n, 32);
+    uint64_t g = ceil_div(nwords, 256);
+    k_lms_list8<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(text, lms, lms_pref, nwords, plist);
+    PSK_KCOUNT();
+    g = ceil_div(n1, 256);
+    k_permute8<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(sa1, n1, plist, out, err);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
 __global__ void k_direct_inverse(const uint32_t *__restrict__ red, uint64_t n1, uint32_t *sa1, uint32_t *err) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t c = red[i];

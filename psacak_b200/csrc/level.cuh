@@ -70,6 +70,13 @@ status_t translate_names(uint32_t *red, uint64_t n1, const uint32_t *types, cons
 status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint32_t *lms_pref, uint64_t n,
                      uint32_t *plist, uint32_t *err, cudaStream_t s);
 
+// Byte levels: out[i] = (P[sa1[i]] << 8) | text[P[sa1[i]] - 1], the permuted
+// LMS positions with their predecessor characters.  `plist` is scratch of
+// n1 entries.
+status_t permute_lms8(const uint32_t *sa1, uint64_t n1, const uint8_t *text, const uint32_t *lms,
+                      const uint32_t *lms_pref, uint64_t n, uint64_t *plist, uint64_t *out, uint32_t *err,
+                      cudaStream_t s);
+
 // Direct inverse when all names are unique: sa1[red[i]] = i.
 status_t direct_inverse(const uint32_t *red, uint64_t n1, uint32_t *sa1, uint32_t *err, cudaStream_t s);
 
