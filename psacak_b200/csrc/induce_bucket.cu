@@ -389,12 +389,20 @@ template <bool LSCAN> struct BucketPolicy {
     uint32_t lms_hi;     // index of this bucket's last entry in that list
     uint32_t lms_cap;    // entries of the list
     uint8_t *c0s;        // c0s[slot] = text[sa[slot] - 1] for every placed entry
-    __device__ __forceinline__ void load(uint64_t i, Item &it, uint32_t &d) const {
+    struct Pre {
+        uint32_t x;
+        uint32_t c0;
+    };
+    __device__ __forceinline__ void pre(uint64_t i, Pre &p) const {
         const uint32_t slot = seq.slot((uint32_t)i);
-        uint32_t x = sa[slot];
+        p.x = sa[slot];
+        p.c0 = c0s[slot];
+    }
+    __device__ __forceinline__ void load(uint64_t i, const Pre &p, Item &it, uint32_t &d) const {
+        const uint32_t x = p.x;
         d = 256;
         if (x > 0) {
-            uint32_t c0 = c0s[slot];
+            uint32_t c0 = p.c0;
             if (LSCAN ? c0 > c : c0 < c) {
                 d = c0;
                 it = (uint64_t)(x - 1) | ((uint64_t)(x >= 2 ? text[x - 2] : 0) << 32);

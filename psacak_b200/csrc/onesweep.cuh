@@ -29,6 +29,8 @@
 //                                      12 / IPT for smaller tiles)
 #pragma once
 
+#include <type_traits>
+
 #include "prims.cuh"
 
 namespace psk {
@@ -87,6 +89,11 @@ __device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile,
     return excl;
 }
 
+// A policy with `using Pre = ...` loads in two phases: pre(i, Pre&) for
+// every item of the thread, then load(i, const Pre&, item, digit).
+template <class P, class = void> struct os_two_phase : std::false_type {};
+template <class P> struct os_two_phase<P, std::void_t<typename P::Pre>> : std::true_type {};
+
 constexpr int os_min_blocks(int at12, int ipt) { return ipt < 12 ? at12 * 12 / ipt : at12; }
 
 template <class Policy, int IPT>
@@ -114,14 +121,31 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
     const uint32_t tile = s_tile;
     const uint64_t base = (uint64_t)tile * TILE;
 
-    // load every item of the thread first (independent loads in flight)
+    // load every item of the thread first (independent loads in flight);
+    // two-phase policies read their direct operands for every item before
+    // any dependent gather
     Item it[IPT];
     uint32_t dg[IPT];
+    if constexpr (os_two_phase<Policy>::value) {
+        typename Policy::Pre pre[IPT];
 #pragma unroll
-    for (int r = 0; r < IPT; r++) {
-        uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
-        dg[r] = 256;
-        if (i < n) pol.load(i, it[r], dg[r]);
+        for (int r = 0; r < IPT; r++) {
+            uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
+            if (i < n) pol.pre(i, pre[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < IPT; r++) {
+            uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
+            dg[r] = 256;
+            if (i < n) pol.load(i, pre[r], it[r], dg[r]);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < IPT; r++) {
+            uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
+            dg[r] = 256;
+            if (i < n) pol.load(i, it[r], dg[r]);
+        }
     }
     // stable ranks within the warp's sub-tile
     uint16_t rk[IPT];
