@@ -212,22 +212,37 @@ __global__ void __launch_bounds__(256) k_keys(const uint32_t *__restrict__ Wg, c
     const int npasses = (nbits + 7) / 8;
     for (int i = threadIdx.x; i < npasses * 256; i += blockDim.x) sh[i] = 0;
     __syncthreads();
+    constexpr int U = 4;  // items per thread step: their rank gathers overlap
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t ib = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); ib < cnt; ib += stride) {
-        const uint64_t i = ib + (threadIdx.x & 31);
-        const bool valid = i < cnt;
-        uint64_t key = 0;
-        if (valid) {
-            const uint32_t v = Wv[i];
-            const uint64_t q = (uint64_t)v + h;
-            uint32_t r = 0;
-            if (q <= n) r = R[q];
-            else dev_fail(err, DEVERR_RANGE);
-            key = ((uint64_t)Wg[i] << KB) | r;
-            keys[i] = key;
-            vals[i] = v;
+    for (uint64_t ib = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); ib < cnt; ib += stride * U) {
+        uint32_t v[U], g[U], r[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = ib + u * stride + (threadIdx.x & 31);
+            v[u] = i < cnt ? Wv[i] : 0u;
+            g[u] = i < cnt ? Wg[i] : 0u;
         }
-        radix_count_digits(sh, key, valid, 0, npasses, nbits);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = ib + u * stride + (threadIdx.x & 31);
+            r[u] = 0;
+            if (i < cnt) {
+                const uint64_t q = (uint64_t)v[u] + h;
+                if (q <= n) r[u] = R[q];
+                else dev_fail(err, DEVERR_RANGE);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = ib + u * stride + (threadIdx.x & 31);
+            const bool valid = i < cnt;
+            const uint64_t key = ((uint64_t)g[u] << KB) | r[u];
+            if (valid) {
+                keys[i] = key;
+                vals[i] = v[u];
+            }
+            radix_count_digits(sh, key, valid, 0, npasses, nbits);
+        }
     }
     __syncthreads();
     radix_flush_digits(sh, npasses, hist);

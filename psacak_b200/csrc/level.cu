@@ -368,14 +368,25 @@ template status_t name_lms<uint32_t>(const uint32_t *, uint64_t, const uint32_t 
 
 __global__ void k_translate(uint32_t *red, uint64_t n1, const uint32_t *__restrict__ types,
                             const uint32_t *__restrict__ heads, uint32_t *err) {
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n1; p += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t c = red[p];
-        if (c >= n1) {
-            dev_fail(err, DEVERR_RANGE);
-            red[p] = 0;
-            continue;
+    constexpr int U = 4;  // symbols per thread step: their gathers overlap
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t p0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p0 < n1; p0 += stride * U) {
+        uint32_t c[U], v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) c[u] = p0 + u * stride < n1 ? red[p0 + u * stride] : 0u;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t p = p0 + u * stride;
+            v[u] = 0;
+            if (p < n1 && c[u] < n1) v[u] = bm_get(types, p) ? heads[c[u] + 1] - 1 : heads[c[u]];
         }
-        red[p] = bm_get(types, p) ? heads[c + 1] - 1 : heads[c];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t p = p0 + u * stride;
+            if (p >= n1) continue;
+            if (c[u] >= n1) dev_fail(err, DEVERR_RANGE);
+            red[p] = v[u];
+        }
     }
 }
 
@@ -404,14 +415,21 @@ __global__ void k_lms_list(const uint32_t *__restrict__ lms, const uint32_t *__r
 }
 
 __global__ void k_permute(uint32_t *sa1, uint64_t n1, const uint32_t *__restrict__ plist, uint32_t *err) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t r = sa1[i];
-        if (r >= n1) {
-            dev_fail(err, DEVERR_RANGE);
-            sa1[i] = 0;
-            continue;
+    constexpr int U = 4;  // entries per thread step: their gathers overlap
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n1; i0 += stride * U) {
+        uint32_t r[U], v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) r[u] = i0 + u * stride < n1 ? sa1[i0 + u * stride] : 0u;
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = r[u] < n1 ? plist[r[u]] : 0u;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = i0 + u * stride;
+            if (i >= n1) continue;
+            if (r[u] >= n1) dev_fail(err, DEVERR_RANGE);
+            sa1[i] = v[u];
         }
-        sa1[i] = plist[r];
     }
 }
 
@@ -448,14 +466,22 @@ __global__ void k_lms_list8(const uint8_t *__restrict__ text, const uint32_t *__
 
 __global__ void k_permute8(const uint32_t *__restrict__ sa1, uint64_t n1, const uint64_t *__restrict__ plist,
                            uint64_t *out, uint32_t *err) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t r = sa1[i];
-        if (r >= n1) {
-            dev_fail(err, DEVERR_RANGE);
-            out[i] = 1ull << 8;
-            continue;
+    constexpr int U = 4;  // entries per thread step: their gathers overlap
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n1; i0 += stride * U) {
+        uint32_t r[U];
+        uint64_t v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) r[u] = i0 + u * stride < n1 ? sa1[i0 + u * stride] : 0u;
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = r[u] < n1 ? plist[r[u]] : (1ull << 8);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t i = i0 + u * stride;
+            if (i >= n1) continue;
+            if (r[u] >= n1) dev_fail(err, DEVERR_RANGE);
+            out[i] = v[u];
         }
-        out[i] = plist[r];
     }
 }
 
