@@ -157,13 +157,104 @@ __global__ void k_init_cursors(const ByteGeom *__restrict__ g, const uint8_t *__
 // The cells of a part (seed q, depth d = 1..runs[q]) go breadth-first: all
 // depth-1 cells in seed order, then depth 2, ...  The cell (q, d) therefore
 // lands at  first + C_1 + ... + C_{d-1} + #{q' < q : runs[q'] >= d},  where
-// C_d = #{q : runs[q] >= d}.  Depths 1..CHAIN_DIRECT are placed straight
-// from one scan over the seeds that counts, per seed, runs >= 1, >= 2, >= 3
-// and the cells deeper than that; only the deep cells (long runs of one
-// character, rare outside runs like N-blocks) go through a sort on depth.
+// C_d = #{q : runs[q] >= d}.
+//
+// Step 1, one look-back scan over the seeds: the load measures each seed's
+// run (the characters c in front of it; c0s already holds the first), the
+// scan counts runs >= 1 and >= 2, and the store places every depth-1 cell and
+// lists the seeds with runs >= 2 as a sub-problem: seed x - 1 with run r - 1,
+// whose cells are exactly the original depths 2, 3, ...  Step 2 solves the
+// (much smaller) sub-list with a four-counter scan that places its depths
+// 1..CHAIN_DIRECT directly; only deeper cells (long runs of one character,
+// such as N-blocks) go through a sort on depth.
 constexpr uint32_t CHAIN_DIRECT = 3;
+constexpr uint32_t CHAIN_CAP = 4;             // run characters measured inside the seed scan
+constexpr uint32_t CHAIN_LONG = 0x80000000u;  // run flag: longer than CHAIN_CAP, not yet measured
 
-// Per-seed counters of the chain scan.
+struct ChainPair {
+    uint32_t c1, c2;
+};
+__device__ __forceinline__ ChainPair shfl_up_t(ChainPair v, int o) {
+    ChainPair r;
+    r.c1 = __shfl_up_sync(FULL_MASK, v.c1, o);
+    r.c2 = __shfl_up_sync(FULL_MASK, v.c2, o);
+    return r;
+}
+struct OpPair {
+    static constexpr int kFields = 2;
+    __device__ __forceinline__ static uint32_t field(int, uint32_t a, uint32_t b) { return a + b; }
+    __device__ __forceinline__ ChainPair operator()(ChainPair a, ChainPair b) const {
+        return ChainPair{a.c1 + b.c1, a.c2 + b.c2};
+    }
+    __device__ __forceinline__ static ChainPair identity() { return ChainPair{0, 0}; }
+};
+
+struct ChainPayload {
+    uint32_t x, r;
+    uint8_t e;
+};
+// Seeds in scan order: L part = sa[start + q]; S part = sa[start - q].
+struct SeedLoad {
+    using Payload = ChainPayload;
+    static constexpr int kIPT = 8;
+    const uint8_t *text;
+    const uint32_t *sa;
+    const uint8_t *c0s;
+    uint32_t start;
+    int dir;
+    uint8_t c;
+    __device__ __forceinline__ ChainPair operator()(uint64_t q, ChainPayload &p) const {
+        const uint32_t slot = dir > 0 ? start + (uint32_t)q : start - (uint32_t)q;
+        const uint32_t x = sa[slot];
+        uint32_t r = 0;
+        uint8_t b = 0;
+        if (x > 0) {
+            b = c0s[slot];
+            if (b == c) {
+                // measured up to CHAIN_CAP characters here; a longer run is
+                // finished by k_chain_totals over the sub-list, so that no
+                // tile waits on a long run (the next tiles' look-back would)
+                r = 1;
+                while (r < x && r < CHAIN_CAP && (b = text[x - r - 1]) == c) r++;
+                if (r == x) b = 0;
+                else if (r == CHAIN_CAP && b == c) r |= CHAIN_LONG;
+            }
+        }
+        p.x = x;
+        p.r = r;
+        p.e = b;
+        const uint32_t rr = r & ~CHAIN_LONG;
+        return ChainPair{rr >= 1 ? 1u : 0u, rr >= 2 ? 1u : 0u};
+    }
+};
+struct SeedStore {
+    uint32_t *sa;
+    uint8_t *c0s;
+    uint32_t *subx, *subr;
+    uint8_t *sube;
+    uint32_t first, limit;  // slot of the first cell; C_1
+    int dir;
+    uint8_t c;
+    uint32_t *err;
+    __device__ __forceinline__ void operator()(uint64_t, ChainPair ex, ChainPair, const ChainPayload &p) const {
+        const uint32_t r = p.r & ~CHAIN_LONG;
+        if (r == 0) return;
+        if (ex.c1 >= limit) {
+            dev_fail(err, DEVERR_RANGE);
+            return;
+        }
+        const uint32_t slot = dir > 0 ? first + ex.c1 : first - ex.c1;
+        sa[slot] = p.x - 1;
+        c0s[slot] = r > 1 ? c : p.e;
+        if (r >= 2) {
+            subx[ex.c2] = p.x - 1;
+            subr[ex.c2] = (r - 1) | (p.r & CHAIN_LONG);  // a long run's length is finished later
+            sube[ex.c2] = p.e;
+        }
+    }
+};
+
+// Per-seed counters of the sub-list scan.
 struct ChainCounts {
     uint32_t c1, c2, c3, deep;
 };
@@ -187,57 +278,28 @@ __device__ __forceinline__ ChainCounts chain_counts(uint32_t r) {
     return ChainCounts{r >= 1 ? 1u : 0u, r >= 2 ? 1u : 0u, r >= 3 ? 1u : 0u, r > CHAIN_DIRECT ? r - CHAIN_DIRECT : 0u};
 }
 
-// Seeds in scan order: L part = sa[start + q]; S part = sa[start - q].
-// runs[q] = number of equal characters c in front of the seed; endc[q] =
-// the character in front of the run.  c0s[slot] (the character in front of
-// sa[slot]) was written beside every seed by whoever placed it, so the text
-// is only read inside runs.  totals[0] = longest run (atomic max),
-// totals[1..4] = the part's ChainCounts (C_1, C_2, C_3, deep cells).
-__global__ void __launch_bounds__(256) k_seed_runs(const uint8_t *__restrict__ text, const uint32_t *__restrict__ sa,
-                                                   uint32_t start, int dir, uint32_t nseeds, uint8_t c,
-                                                   uint32_t *runs, uint32_t *totals, const uint8_t *c0s,
-                                                   uint8_t *endc) {
+// Totals of a sub-list: totals[0] = longest run (atomic max), totals[1..4] =
+// its ChainCounts sums.  Runs flagged CHAIN_LONG are measured to the end
+// first (seed x = xs[q] has at least the flagged length of c in front).
+__global__ void __launch_bounds__(256) k_chain_totals(const uint8_t *__restrict__ text, const uint32_t *__restrict__ xs,
+                                                      uint32_t *runs, uint8_t *endc, uint8_t c, uint32_t m,
+                                                      uint32_t *totals) {
     __shared__ uint32_t s_red[8][5];
-    constexpr int U = 4;  // seeds per thread step: their loads and first gathers overlap
     uint32_t mx = 0;
     ChainCounts acc{0, 0, 0, 0};
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint64_t q0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q0 < nseeds; q0 += (uint64_t)stride * U) {
-        uint32_t x[U], slot[U];
-        uint8_t before[U], nxt[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const uint64_t q = q0 + (uint64_t)u * stride;
-            slot[u] = dir > 0 ? start + (uint32_t)q : start - (uint32_t)q;
-            x[u] = q < nseeds ? sa[slot[u]] : 0u;
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) before[u] = x[u] > 0 ? c0s[slot[u]] : 0;
-#pragma unroll
-        for (int u = 0; u < U; u++) nxt[u] = (before[u] == c && x[u] >= 2) ? text[x[u] - 2] : 0;
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const uint64_t q = q0 + (uint64_t)u * stride;
-            if (q >= nseeds) continue;
-            uint32_t r = 0;
-            uint8_t b = before[u];
-            if (x[u] > 0 && b == c) {
-                // the run holds x-1; nxt = text[x-2] is already here
-                r = 1;
-                if (r < x[u]) {
-                    b = nxt[u];
-                    if (b == c) {
-                        r = 2;
-                        while (r < x[u] && (b = text[x[u] - r - 1]) == c) r++;
-                    }
-                }
-                if (r == x[u]) b = 0;
-            }
-            endc[q] = b;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+        uint32_t r = runs[q];
+        if (r & CHAIN_LONG) {
+            const uint32_t x = xs[q];
+            r &= ~CHAIN_LONG;
+            uint8_t b = c;
+            while (r < x && (b = text[x - r - 1]) == c) r++;
+            if (r == x) b = 0;
             runs[q] = r;
-            mx = r > mx ? r : mx;
-            acc = OpChain()(acc, chain_counts(r));
+            endc[q] = b;
         }
+        mx = r > mx ? r : mx;
+        acc = OpChain()(acc, chain_counts(r));
     }
     for (int o = 16; o > 0; o >>= 1) {
         uint32_t t = __shfl_down_sync(FULL_MASK, mx, o);
@@ -269,24 +331,17 @@ __global__ void __launch_bounds__(256) k_seed_runs(const uint8_t *__restrict__ t
     }
 }
 
-// Chain scan: per seed its ChainCounts; the load also fetches the seed, its
-// run length and the character in front of its run, and the store writes
-// the seed's cells of depth 1..3 (entry and predecessor character) and the
-// offset of its deep cells.
-struct ChainPayload {
-    uint32_t x, r;
-    uint8_t e;
-};
+// Sub-list scan: per seed its ChainCounts; the store writes the seed's cells
+// of depth 1..3 (entry and predecessor character) and the offset of its
+// deep cells.
 struct ChainLoad {
     using Payload = ChainPayload;
     static constexpr int kIPT = 6;
-    const uint32_t *sa;
+    const uint32_t *xs;
     const uint32_t *runs;
     const uint8_t *endc;
-    uint32_t start;
-    int dir;
     __device__ __forceinline__ ChainCounts operator()(uint64_t q, ChainPayload &p) const {
-        p.x = sa[dir > 0 ? start + (uint32_t)q : start - (uint32_t)q];
+        p.x = xs[q];
         p.r = runs[q];
         p.e = endc[q];
         return chain_counts(p.r);
@@ -295,7 +350,7 @@ struct ChainLoad {
 struct ChainStore {
     uint32_t *sa;
     uint8_t *c0s;
-    uint32_t *deep_off;  // null when the part has no deep cells
+    uint32_t *deep_off;  // null when the sub-list has no deep cells
     uint32_t first;      // slot of the first cell
     uint32_t base2, base3;  // C_1 and C_1 + C_2
     uint32_t limit;         // cells of depth <= 3 (C_1 + C_2 + C_3)
@@ -320,12 +375,11 @@ struct ChainStore {
     }
 };
 
-// Deep cell q (row-major over seeds, depths > 3) -> (depth - 3, value
-// (seed - depth) << 8 | the character in front of that suffix).
-__global__ void k_expand_deep(const uint32_t *__restrict__ sa, uint32_t start, int dir, uint32_t nseeds,
-                              const uint32_t *__restrict__ off, const uint32_t *__restrict__ runs,
-                              const uint8_t *__restrict__ endc, uint8_t c, uint32_t ncells, uint32_t *keys,
-                              uint64_t *vals) {
+// Deep cell q (row-major over sub-list seeds, depths > 3) -> (depth - 3,
+// value (seed - depth) << 8 | the character in front of that suffix).
+__global__ void k_expand_deep(const uint32_t *__restrict__ xs, uint32_t nseeds, const uint32_t *__restrict__ off,
+                              const uint32_t *__restrict__ runs, const uint8_t *__restrict__ endc, uint8_t c,
+                              uint32_t ncells, uint32_t *keys, uint64_t *vals) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ncells; q += gridDim.x * blockDim.x) {
         // last seed s with off[s] <= q (seeds without deep cells share the next one's offset)
         uint32_t lo = 0, hi = nseeds - 1;
@@ -336,7 +390,7 @@ __global__ void k_expand_deep(const uint32_t *__restrict__ sa, uint32_t start, i
         }
         uint32_t dd = q - off[lo] + 1;
         uint32_t d = dd + CHAIN_DIRECT;
-        uint32_t x = sa[dir > 0 ? start + lo : start - lo];
+        uint32_t x = xs[lo];
         uint8_t pc = d < runs[lo] ? c : endc[lo];
         keys[q] = dd;
         vals[q] = ((uint64_t)(x - d) << 8) | pc;
@@ -449,38 +503,51 @@ static inline uint32_t grid_cap(uint64_t n, uint32_t cap) {
 // seed in scan order, `nseeds` the seeds present, `part` the full size of
 // the part; fills the remaining part - nseeds slots.
 static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint32_t start, int dir, uint32_t nseeds,
-                              uint32_t part, uint8_t c, uint32_t *runs, uint32_t *off, uint8_t *endc, uint8_t *c0s,
-                              uint32_t *k0, uint64_t *v0, uint32_t *k1, uint64_t *v1, cudaStream_t s) {
+                              uint32_t part, uint8_t c, uint32_t *subx, uint32_t *subr, uint8_t *sube, uint32_t *off,
+                              uint8_t *c0s, uint32_t *k0, uint64_t *v0, uint32_t *k1, uint64_t *v1, cudaStream_t s) {
     if (part == 0) return PSACAK_OK;
     if (nseeds == 0 || nseeds > part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds for a part of %u", c, nseeds, part);
-    uint32_t *d_tot = ctx.d_scalars + 24;  // [max run, C_1, C_2, C_3, deep cells]
-    PSK_CUDA(cudaMemsetAsync(d_tot, 0, 5 * sizeof(uint32_t), s));
-    PSK_PROF_LAUNCH(s, "chain_runs", nseeds, 0,
-                    (k_seed_runs<<<grid_cap(nseeds, 4096), 256, 0, s>>>(text, sa, start, dir, nseeds, c, runs, d_tot,
-                                                                         c0s, endc)));
-    if (nseeds == part) return PSACAK_OK;
-    uint32_t h[5];
-    PSK_TRY(ctx.read_u32(d_tot, h, 5));
-    const uint32_t maxrun = h[0], C1 = h[1], C2 = h[2], C3 = h[3], ndeep = h[4];
-    const uint64_t ncells = (uint64_t)C1 + C2 + C3 + ndeep;
-    if (nseeds + ncells != part)
-        return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds + %llu chained != %u", c, nseeds,
-                         (unsigned long long)ncells, part);
+    if (nseeds == part) return PSACAK_OK;  // nothing chained: no seed has c in front of it
     const uint32_t first = dir > 0 ? start + nseeds : start - nseeds;
-    const uint32_t direct = C1 + C2 + C3;
-    PSK_TRY((ctx.scan<ChainCounts, OpChain>(ChainLoad{sa, runs, endc, start, dir},
-                                            ChainStore{sa, c0s, ndeep ? off : nullptr, first, C1, C1 + C2, direct, dir,
+    const uint32_t cells = part - nseeds;
+    // step 1: depth-1 cells and the sub-list of runs >= 2
+    ChainPair *d_pair = (ChainPair *)(ctx.d_scalars + 24);
+    PSK_TRY((ctx.scan<ChainPair, OpPair>(SeedLoad{text, sa, c0s, start, dir, c},
+                                         SeedStore{sa, c0s, subx, subr, sube, first, cells, dir, c, ctx.d_err}, nseeds,
+                                         d_pair, OpPair(), "chain_seeds")));
+    uint32_t h[5];
+    PSK_TRY(ctx.read_u32((const uint32_t *)d_pair, h, 2));
+    const uint32_t C1 = h[0], m = h[1];
+    if (m == 0) {
+        if (C1 != cells) return set_error(PSACAK_EINTERNAL, "bucket %u: %u chained != %u", c, C1, cells);
+        return PSACAK_OK;
+    }
+    // step 2: the sub-list (seeds x - 1 with runs r - 1) from slot first + C1
+    uint32_t *d_tot = ctx.d_scalars + 26;  // [max run, C'_1, C'_2, C'_3, deep cells]
+    PSK_CUDA(cudaMemsetAsync(d_tot, 0, 5 * sizeof(uint32_t), s));
+    PSK_PROF_LAUNCH(s, "chain_totals", m, 0,
+                    (k_chain_totals<<<grid_cap(m, 1184), 256, 0, s>>>(text, subx, subr, sube, c, m, d_tot)));
+    PSK_TRY(ctx.read_u32(d_tot, h, 5));
+    const uint32_t maxrun = h[0], D1 = h[1], D2 = h[2], D3 = h[3], ndeep = h[4];
+    if ((uint64_t)C1 + D1 + D2 + D3 + ndeep != cells || D1 != m)
+        return set_error(PSACAK_EINTERNAL, "bucket %u: %u + %u + %u + %u + %u chained != %u", c, C1, D1, D2, D3, ndeep,
+                         cells);
+    const uint32_t sfirst = dir > 0 ? first + C1 : first - C1;
+    const uint32_t direct = D1 + D2 + D3;
+    PSK_TRY((ctx.scan<ChainCounts, OpChain>(ChainLoad{subx, subr, sube},
+                                            ChainStore{sa, c0s, ndeep ? off : nullptr, sfirst, D1, D1 + D2, direct, dir,
                                                        c, ctx.d_err},
-                                            nseeds, (ChainCounts *)nullptr, OpChain(), "chain_place")));
+                                            m, (ChainCounts *)nullptr, OpChain(), "chain_place")));
     if (ndeep == 0) return PSACAK_OK;
+    // step 3: cells deeper than the direct depths, sorted on depth
     PSK_PROF_LAUNCH(s, "chain_deep", ndeep, 0,
-                    (k_expand_deep<<<grid_cap(ndeep, 8192), 256, 0, s>>>(sa, start, dir, nseeds, off, runs, endc, c,
-                                                                           ndeep, k0, v0)));
+                    (k_expand_deep<<<grid_cap(ndeep, 8192), 256, 0, s>>>(subx, m, off, subr, sube, c, ndeep, k0,
+                                                                           v0)));
     PSK_LAUNCH_CHECK();
     int in1 = 0;
     PSK_TRY((ctx.radix_sort<uint32_t, uint64_t>(k0, v0, k1, v1, ndeep, 0, bitlen(maxrun - CHAIN_DIRECT), &in1)));
-    const uint32_t dfirst = dir > 0 ? first + direct : first - direct;
+    const uint32_t dfirst = dir > 0 ? sfirst + direct : sfirst - direct;
     PSK_PROF_LAUNCH(s, "chain_place_deep", ndeep, 13ull * ndeep,
                     (k_place_cells<<<grid_cap(ndeep, 8192), 256, 0, s>>>(in1 ? v1 : v0, ndeep, dfirst, dir, sa, c0s)));
     PSK_LAUNCH_CHECK();
@@ -518,7 +585,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         maxpart = hg.lcount[c] > maxpart ? hg.lcount[c] : maxpart;
         maxpart = hg.scount[c] > maxpart ? hg.scount[c] : maxpart;
     }
-    DBuf<uint32_t> cur, cur2, runs, off, k0, k1;
+    DBuf<uint32_t> cur, cur2, runs, off, k0, k1, subx;
     DBuf<uint64_t> v0, v1;
     DBuf<uint8_t> endc, c0s;
     PSK_TRY(cur.init(ctx, 512));
@@ -526,6 +593,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
     PSK_TRY(endc.init(ctx, maxpart));
     PSK_TRY(c0s.init(ctx, n));
     PSK_TRY(runs.init(ctx, maxpart));
+    PSK_TRY(subx.init(ctx, maxpart));
     PSK_TRY(off.init(ctx, maxpart));
     PSK_TRY(k0.init(ctx, maxpart));
     PSK_TRY(v0.init(ctx, maxpart));
@@ -560,8 +628,8 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (lc > 0) {
             uint32_t cl = 0;
             PSK_TRY(ctx.read_u32(curL + c, &cl));
-            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, runs, off, endc, c0s, k0, v0, k1,
-                                  v1, s));
+            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, subx, runs, endc, off, c0s, k0,
+                                  v0, k1, v1, s));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
         PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, c0s, s));
@@ -576,8 +644,8 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (sc > 0) {
             uint32_t cs = 0;
             PSK_TRY(ctx.read_u32(curS + c, &cs));
-            PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, runs, off, endc, c0s, k0, v0,
-                                  k1, v1, s));
+            PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, subx, runs, endc, off, c0s,
+                                  k0, v0, k1, v1, s));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
         const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;
