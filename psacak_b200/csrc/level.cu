@@ -65,12 +65,12 @@ __global__ void __launch_bounds__(TYPE_BLOCK) k_type_main(const C *__restrict__ 
                                                           uint32_t *__restrict__ lms_wcnt, ByteHist *ghist) {
     __shared__ uint32_t s_scan[33];
     __shared__ uint32_t s_hi[TYPE_BLOCK];
-    __shared__ uint32_t s_hist[HIST ? 3 * 256 : 1];
+    __shared__ uint32_t s_hist[HIST ? (TYPE_BLOCK / 32) * 3 * 256 : 1];
     const int w = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t nwords = ceil_div(n, 32);
     if (HIST)
-        for (int i = threadIdx.x; i < 3 * 256; i += TYPE_BLOCK) s_hist[i] = 0;
+        for (int i = threadIdx.x; i < (TYPE_BLOCK / 32) * 3 * 256; i += TYPE_BLOCK) s_hist[i] = 0;
 
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t tstart = tile * TYPE_TILE;
@@ -142,22 +142,19 @@ __global__ void __launch_bounds__(TYPE_BLOCK) k_type_main(const C *__restrict__ 
             lms_wcnt[wg] = __popc(Lm);
         }
         if (HIST) {
+            // per-warp private histograms: lanes add their own position
+            // (conflicts only among the lanes of one warp)
+            uint32_t *wh = s_hist + w * 3 * 256;
 #pragma unroll
             for (int it = 0; it < 32; it++) {
-                uint32_t Tw = __shfl_sync(FULL_MASK, T, it);
-                uint32_t Lw = __shfl_sync(FULL_MASK, Lm, it);
-                uint64_t p = tstart + (uint64_t)(w * 32 + it) * 32 + lane;
-                bool valid = p < n;
-                uint32_t a = (pk[it >> 2] >> ((it & 3) * 8)) & 0xFFu;
-                uint32_t key = valid ? a : 256u;
-                uint32_t peers = __match_any_sync(FULL_MASK, key);
-                uint32_t lb = __ballot_sync(FULL_MASK, valid && !((Tw >> lane) & 1u));
-                uint32_t mb = __ballot_sync(FULL_MASK, valid && ((Lw >> lane) & 1u));
-                if (valid && (int)lane == __ffs(peers) - 1) {
-                    atomicAdd(&s_hist[a], __popc(peers));
-                    uint32_t nl = __popc(peers & lb), nm = __popc(peers & mb);
-                    if (nl) atomicAdd(&s_hist[256 + a], nl);
-                    if (nm) atomicAdd(&s_hist[512 + a], nm);
+                const uint32_t Tw = __shfl_sync(FULL_MASK, T, it);
+                const uint32_t Lw = __shfl_sync(FULL_MASK, Lm, it);
+                const uint64_t p = tstart + (uint64_t)(w * 32 + it) * 32 + lane;
+                if (p < n) {
+                    const uint32_t a = (pk[it >> 2] >> ((it & 3) * 8)) & 0xFFu;
+                    atomicAdd(&wh[a], 1u);
+                    if (!((Tw >> lane) & 1u)) atomicAdd(&wh[256 + a], 1u);
+                    if ((Lw >> lane) & 1u) atomicAdd(&wh[512 + a], 1u);
                 }
             }
         }
@@ -166,9 +163,15 @@ __global__ void __launch_bounds__(TYPE_BLOCK) k_type_main(const C *__restrict__ 
     if (HIST) {
         __syncthreads();
         for (int i = threadIdx.x; i < 256; i += TYPE_BLOCK) {
-            if (s_hist[i]) atomicAdd(&ghist->count[i], s_hist[i]);
-            if (s_hist[256 + i]) atomicAdd(&ghist->lcount[i], s_hist[256 + i]);
-            if (s_hist[512 + i]) atomicAdd(&ghist->lmscount[i], s_hist[512 + i]);
+            uint32_t a = 0, b = 0, m = 0;
+            for (int ww = 0; ww < TYPE_BLOCK / 32; ww++) {
+                a += s_hist[ww * 768 + i];
+                b += s_hist[ww * 768 + 256 + i];
+                m += s_hist[ww * 768 + 512 + i];
+            }
+            if (a) atomicAdd(&ghist->count[i], a);
+            if (b) atomicAdd(&ghist->lcount[i], b);
+            if (m) atomicAdd(&ghist->lmscount[i], m);
         }
     }
 }
