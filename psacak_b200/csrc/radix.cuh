@@ -108,8 +108,18 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
 #pragma unroll
     for (int r = 0; r < IPT; r++) {
         const uint32_t idx = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
-        const uint32_t d = idx < cnt ? (uint32_t)(s_k[idx] >> shift) & dmask : 256u;
-        const uint32_t peers = __match_any_sync(FULL_MASK, d);
+        const bool valid = idx < cnt;
+        const uint32_t d = valid ? (uint32_t)(s_k[idx] >> shift) & dmask : 256u;
+        // lanes with the same digit: the intersection of eight bit ballots
+        // (ALU votes instead of one match.any through the MIO pipe)
+        uint32_t peers = __ballot_sync(FULL_MASK, valid);
+        if (!valid) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const uint32_t bit = (d >> b) & 1u;
+            const uint32_t bb = __ballot_sync(FULL_MASK, bit);
+            peers &= bit ? bb : ~bb;
+        }
         const uint32_t prior = d < 256 ? s_wcnt[w][d] : 0u;
         rd[r] = ((prior + __popc(peers & lt)) << 9) | d;
         __syncwarp();
