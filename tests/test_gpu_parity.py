@@ -56,6 +56,26 @@ def test_edge_cases(ctx, engine):
         assert (ctx.psacak(a, sched(engine)) == o.psacak8(a)).all(), t[:20]
 
 
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_runs_of_every_length(ctx, seed):
+    """Runs of one character of every length around the chain scan's direct
+    depths and its in-scan measuring cap (1..12), plus runs of hundreds to
+    tens of thousands (measured after the scan), mixed in random order, so
+    that bucket parts hold seeds of every depth and deep cells."""
+    rng = np.random.default_rng(seed)
+    pieces = []
+    for _ in range(3000):
+        c = rng.integers(0, 4)
+        k = int(rng.integers(1, 13)) if rng.random() < 0.97 else int(rng.integers(100, 20000))
+        pieces.append(np.full(k, [65, 67, 71, 84][c], np.uint8))
+        if rng.random() < 0.3:
+            pieces.append(rng.integers(65, 69, int(rng.integers(1, 4))).astype(np.uint8))
+    t = np.concatenate(pieces)
+    want = o.psacak8(t)
+    for engine in ENGINES:
+        assert (ctx.psacak(t, sched(engine)) == want).all(), engine
+
+
 @pytest.mark.parametrize("engine", ENGINES)
 def test_random_small_u8(ctx, engine):
     rng = np.random.default_rng(20)
