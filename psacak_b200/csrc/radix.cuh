@@ -109,7 +109,10 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
     for (int r = 0; r < IPT; r++) {
         const uint32_t idx = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
         const bool valid = idx < cnt;
-        const uint32_t d = valid ? (uint32_t)(s_k[idx] >> shift) & dmask : 256u;
+        // the digit lies in one 32-bit half of the key (shift is a multiple of 8)
+        const uint32_t half = sizeof(K) == 8 ? reinterpret_cast<const uint32_t *>(s_k)[2 * idx + (shift >> 5)]
+                                             : (uint32_t)s_k[idx];
+        const uint32_t d = valid ? (half >> (shift & 31)) & dmask : 256u;
         // lanes with the same digit: the intersection of eight bit ballots
         // (ALU votes instead of one match.any through the MIO pipe)
         uint32_t peers = __ballot_sync(FULL_MASK, valid);
