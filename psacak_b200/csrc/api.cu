@@ -487,7 +487,14 @@ status_t ctx_init(Ctx &c, int device) {
     c.dev.smem_optin = prop.sharedMemPerBlockOptin;
     PSK_CUDA(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
     c.stream = c.own_stream;
-    PSK_CUDA(cudaDeviceGetDefaultMemPool(&c.pool, device));
+    // A pool of the context's own (the device's default pool, shared with the
+    // application, keeps its settings): it keeps freed memory for reuse
+    // within a build and is trimmed whenever the arena is regrown.
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    PSK_CUDA(cudaMemPoolCreate(&c.pool, &props));
     uint64_t thresh = UINT64_MAX;
     PSK_CUDA(cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh));
     PSK_CUDA(cudaMallocHost(&c.h_pinned, 4096));
@@ -523,6 +530,9 @@ void ctx_free(Ctx &c) {
     if (c.d_induced) cudaFree(c.d_induced);
     if (c.arena) cudaFree(c.arena);
     c.arena = nullptr;
+    if (c.own_stream) cudaStreamSynchronize(c.own_stream);
+    if (c.pool) cudaMemPoolDestroy(c.pool);
+    c.pool = nullptr;
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
     c.h_pinned = nullptr;
 }
@@ -850,8 +860,10 @@ int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *
     }
     uint8_t *dt = nullptr;
     uint32_t *ds = nullptr;
-    PSK_CUDA(cudaMallocAsync(&dt, off[n_texts], c.own_stream));
-    st = cudaMallocAsync(&ds, off[n_texts] * sizeof(uint32_t), c.own_stream) == cudaSuccess ? PSACAK_OK : PSACAK_ENOMEM;
+    PSK_CUDA(cudaMallocFromPoolAsync(&dt, off[n_texts], c.pool, c.own_stream));
+    st = cudaMallocFromPoolAsync(&ds, off[n_texts] * sizeof(uint32_t), c.pool, c.own_stream) == cudaSuccess
+             ? PSACAK_OK
+             : PSACAK_ENOMEM;
     if (st == PSACAK_OK) {
         for (uint32_t i = 0; i < n_texts && st == PSACAK_OK; i++)
             if (lens[i] && cudaMemcpyAsync(dt + off[i], texts[i], lens[i], cudaMemcpyHostToDevice, c.own_stream) !=

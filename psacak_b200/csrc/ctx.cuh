@@ -68,6 +68,8 @@ struct Ctx {
             if (arena) cudaFree(arena);
             arena = nullptr;
             arena_size = 0;
+            // what the pool kept from the builds that outgrew the arena goes back
+            PSK_CUDA(cudaMemPoolTrimTo(pool, 0));
             size_t want = arena_high + arena_high / 8 + (64u << 20);
             PSK_CUDA(cudaMalloc(&arena, want));
             arena_size = want;
@@ -130,7 +132,9 @@ struct Ctx {
         struct timespec ts;
         clock_gettime(CLOCK_MONOTONIC, &ts);
         double t = ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
-        if (stage_t0 > 0) fprintf(stderr, "[psacak] level %u %-24s %9.3f ms\n", level, what, t - stage_t0);
+        if (stage_t0 > 0)
+            fprintf(stderr, "[psacak] level %u %-24s %9.3f ms  workspace %.2f GB (peak %.2f GB)\n", level, what,
+                    t - stage_t0, arena_vtop / 1e9, arena_high / 1e9);
         stage_t0 = t;
     }
     // Items per thread of the bucket scans' scatter and of the compactions
@@ -146,7 +150,7 @@ struct Ctx {
         if (os.status) cudaFreeAsync(os.status, stream);
         os.status = nullptr;
         os.max_tiles = 0;
-        PSK_CUDA(cudaMallocAsync(&os.status, want * 256 * sizeof(uint64_t), stream));
+        PSK_CUDA(cudaMallocFromPoolAsync(&os.status, want * 256 * sizeof(uint64_t), pool, stream));
         // zeroed words read as "not ready" for every epoch
         PSK_CUDA(cudaMemsetAsync(os.status, 0, want * 256 * sizeof(uint64_t), stream));
         os.max_tiles = want;
@@ -160,7 +164,7 @@ struct Ctx {
         if (ss.flags) cudaFreeAsync(ss.flags, stream);
         ss.flags = nullptr;
         ss.max_tiles = 0;
-        PSK_CUDA(cudaMallocAsync(&ss.flags, want * LS_MAX_FIELDS * sizeof(uint64_t), stream));
+        PSK_CUDA(cudaMallocFromPoolAsync(&ss.flags, want * LS_MAX_FIELDS * sizeof(uint64_t), pool, stream));
         // zeroed words read as "not ready" for every epoch
         PSK_CUDA(cudaMemsetAsync(ss.flags, 0, want * LS_MAX_FIELDS * sizeof(uint64_t), stream));
         ss.max_tiles = want;

@@ -504,7 +504,7 @@ static inline uint32_t grid_cap(uint64_t n, uint32_t cap) {
 // the part; fills the remaining part - nseeds slots.
 static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint32_t start, int dir, uint32_t nseeds,
                               uint32_t part, uint8_t c, uint32_t *subx, uint32_t *subr, uint8_t *sube, uint32_t *off,
-                              uint8_t *c0s, uint32_t *k0, uint64_t *v0, uint32_t *k1, uint64_t *v1, cudaStream_t s) {
+                              uint8_t *c0s, cudaStream_t s) {
     if (part == 0) return PSACAK_OK;
     if (nseeds == 0 || nseeds > part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds for a part of %u", c, nseeds, part);
@@ -540,16 +540,25 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
                                                        c, ctx.d_err},
                                             m, (ChainCounts *)nullptr, OpChain(), "chain_place")));
     if (ndeep == 0) return PSACAK_OK;
-    // step 3: cells deeper than the direct depths, sorted on depth
+    // step 3: cells deeper than the direct depths, sorted on depth (buffers
+    // sized to this part's deep cells)
+    DBuf<uint32_t> k0, k1;
+    DBuf<uint64_t> v0, v1;
+    PSK_TRY(k0.init(ctx, ndeep));
+    PSK_TRY(k1.init(ctx, ndeep));
+    PSK_TRY(v0.init(ctx, ndeep));
+    PSK_TRY(v1.init(ctx, ndeep));
     PSK_PROF_LAUNCH(s, "chain_deep", ndeep, 0,
                     (k_expand_deep<<<grid_cap(ndeep, 8192), 256, 0, s>>>(subx, m, off, subr, sube, c, ndeep, k0,
                                                                            v0)));
     PSK_LAUNCH_CHECK();
     int in1 = 0;
-    PSK_TRY((ctx.radix_sort<uint32_t, uint64_t>(k0, v0, k1, v1, ndeep, 0, bitlen(maxrun - CHAIN_DIRECT), &in1)));
+    PSK_TRY((ctx.radix_sort<uint32_t, uint64_t>(k0.get(), v0.get(), k1.get(), v1.get(), ndeep, 0,
+                                                bitlen(maxrun - CHAIN_DIRECT), &in1)));
     const uint32_t dfirst = dir > 0 ? sfirst + direct : sfirst - direct;
     PSK_PROF_LAUNCH(s, "chain_place_deep", ndeep, 13ull * ndeep,
-                    (k_place_cells<<<grid_cap(ndeep, 8192), 256, 0, s>>>(in1 ? v1 : v0, ndeep, dfirst, dir, sa, c0s)));
+                    (k_place_cells<<<grid_cap(ndeep, 8192), 256, 0, s>>>(in1 ? v1.get() : v0.get(), ndeep, dfirst, dir,
+                                                                          sa, c0s)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -585,8 +594,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         maxpart = hg.lcount[c] > maxpart ? hg.lcount[c] : maxpart;
         maxpart = hg.scount[c] > maxpart ? hg.scount[c] : maxpart;
     }
-    DBuf<uint32_t> cur, cur2, runs, off, k0, k1, subx;
-    DBuf<uint64_t> v0, v1;
+    DBuf<uint32_t> cur, cur2, runs, off, subx;
     DBuf<uint8_t> endc, c0s;
     PSK_TRY(cur.init(ctx, 512));
     PSK_TRY(cur2.init(ctx, 512));
@@ -595,10 +603,6 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
     PSK_TRY(runs.init(ctx, maxpart));
     PSK_TRY(subx.init(ctx, maxpart));
     PSK_TRY(off.init(ctx, maxpart));
-    PSK_TRY(k0.init(ctx, maxpart));
-    PSK_TRY(v0.init(ctx, maxpart));
-    PSK_TRY(k1.init(ctx, maxpart));
-    PSK_TRY(v1.init(ctx, maxpart));
     uint32_t *curL = cur.get(), *curS = cur.get() + 256;
     uint32_t *alt = cur2.get();
 
@@ -628,8 +632,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (lc > 0) {
             uint32_t cl = 0;
             PSK_TRY(ctx.read_u32(curL + c, &cl));
-            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, subx, runs, endc, off, c0s, k0,
-                                  v0, k1, v1, s));
+            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, subx, runs, endc, off, c0s, s));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
         PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, c0s, s));
@@ -645,7 +648,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
             uint32_t cs = 0;
             PSK_TRY(ctx.read_u32(curS + c, &cs));
             PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, subx, runs, endc, off, c0s,
-                                  k0, v0, k1, v1, s));
+                                  s));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
         const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;

@@ -359,6 +359,14 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
     const int KB = bitlen(n);
     uint64_t ngroups = nbuckets;
     Tri *d_tri = (Tri *)(ctx.d_scalars + 4);
+    // The work list (Wg, Wv) lives as two u32 arrays inside the key array of
+    // the radix pair that is spare: it enters in (k1, v1), the keys are built
+    // into the other pair, and each round writes the next list into whichever
+    // pair the sort did not leave its result in.
+    uint64_t *kA = k0, *kB = k1;
+    uint32_t *vA = v0, *vB = v1;
+    if (Wg != (uint32_t *)k1 || Wv != Wg + n)
+        return set_error(PSACAK_EINTERNAL, "doubling rounds: work list outside its radix pair");
     for (uint64_t h = 1; cnt > 0; h <<= 1) {
         const int GB = bitlen(ngroups > 0 ? ngroups - 1 : 0);
         if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
@@ -366,15 +374,21 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
         PSK_CUDA(cudaMemsetAsync(ctx.d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
         PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
                         (k_keys<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
-                            Wg, Wv, cnt, R, n, h, KB, k0, v0, KB + GB, ctx.d_hist, ctx.d_err)));
+                            Wg, Wv, cnt, R, n, h, KB, kA, vA, KB + GB, ctx.d_hist, ctx.d_err)));
         PSK_LAUNCH_CHECK();
         int in1 = 0;
-        PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(k0, v0, k1, v1, cnt, 0, KB + GB, &in1, true)));
-        const uint64_t *ks = in1 ? k1 : k0;
-        const uint32_t *vs = in1 ? v1 : v0;
+        PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(kA, vA, kB, vB, cnt, 0, KB + GB, &in1, true)));
+        uint64_t *ks = in1 ? kB : kA, *kfree = in1 ? kA : kB;
+        uint32_t *vs = in1 ? vB : vA, *vfree = in1 ? vA : vB;
+        Wg = (uint32_t *)kfree;
+        Wv = Wg + n;
         PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, ngroups, KB, ctx.d_err},
                                       RoundStore{gB, R, sa, Wg, Wv, n, ctx.d_err}, cnt, d_tri, OpTri(),
                                       "scan_rounds")));
+        kA = ks;
+        vA = vs;
+        kB = kfree;
+        vB = vfree;
         uint32_t tri[4];
         PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
         if (ctx.stage_timing)
@@ -391,19 +405,18 @@ template <class C>
 status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
                          Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
                          uint32_t *cursor, uint32_t *sa, cudaStream_t s) {
-    DBuf<uint32_t> R, Wg, Wv, v0, v1, gA, gB;
+    DBuf<uint32_t> R, v0, v1, gA, gB;
     DBuf<uint64_t> k0, k1;
     // group-start tables: indexed by bucket id (round 1) or kept-group ordinal
     const uint64_t gcap = n > nbuckets ? n : nbuckets;
     PSK_TRY(gA.init(ctx, gcap));
     PSK_TRY(gB.init(ctx, gcap));
     PSK_TRY(R.init(ctx, n + 1));
-    PSK_TRY(Wg.init(ctx, n));
-    PSK_TRY(Wv.init(ctx, n));
     PSK_TRY(v0.init(ctx, n));
     PSK_TRY(v1.init(ctx, n));
     PSK_TRY(k0.init(ctx, n));
     PSK_TRY(k1.init(ctx, n));
+    uint32_t *Wg = (uint32_t *)k1.get(), *Wv = Wg + n;  // the work list (see doubling_rounds)
     PSK_CUDA(cudaMemsetAsync(R.get() + n, 0, sizeof(uint32_t), s));  // the sentinel ranks lowest
     const uint64_t nwords = ceil_div(n, 32);
     if (mode == INDUCE_LMS_SUBSTRINGS) {
@@ -428,18 +441,17 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
 // for short strings, where it replaces the remaining recursion levels.
 status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bheads, uint64_t nbuckets, uint64_t n,
                           uint32_t *sa, cudaStream_t s) {
-    DBuf<uint32_t> R, Wg, Wv, v0, v1, gA, gB;
+    DBuf<uint32_t> R, v0, v1, gA, gB;
     DBuf<uint64_t> k0, k1;
     const uint64_t gcap = n > nbuckets ? n : nbuckets;
     PSK_TRY(gA.init(ctx, gcap));
     PSK_TRY(gB.init(ctx, gcap));
     PSK_TRY(R.init(ctx, n + 1));
-    PSK_TRY(Wg.init(ctx, n));
-    PSK_TRY(Wv.init(ctx, n));
     PSK_TRY(v0.init(ctx, n));
     PSK_TRY(v1.init(ctx, n));
     PSK_TRY(k0.init(ctx, n));
     PSK_TRY(k1.init(ctx, n));
+    uint32_t *Wg = (uint32_t *)k1.get(), *Wv = Wg + n;  // the work list (see doubling_rounds)
     PSK_CUDA(cudaMemsetAsync(R.get() + n, 0, sizeof(uint32_t), s));
     uint64_t gb = ceil_div(nbuckets, 256);
     k_copy_heads<<<(uint32_t)(gb < 4096 ? gb : 4096), 256, 0, s>>>(bheads, nbuckets, gA);
