@@ -24,6 +24,12 @@
 #include <map>
 #include <vector>
 
+/* The pipelined scans of the reference's par_induce_sort (psacak_oracle_par.cpp). */
+namespace oracle_par {
+void induce_sort8_par(const uint8_t *text, size_t len, uint32_t *suf, uint32_t *ptrs_head, uint32_t *ptrs_tail,
+                      bool left_most, unsigned threads);
+}
+
 namespace {
 
 typedef unsigned __int128 u128;
@@ -573,8 +579,17 @@ void induce_sort8(const uint8_t *text, size_t len, uint32_t *suf, Buckets &bkt,
     }
 }
 
+/* src/psacak8.rs:108-123 induce_sort: the pipelined scans from two blocks of
+ * 128Ki up when threads are given, else the serial ones. */
+void induce_sort8_any(const uint8_t *text, size_t len, uint32_t *suf, Buckets &bkt, bool left_most,
+                      unsigned threads) {
+    if (threads > 0 && len >= 2 * 128 * 1024)
+        oracle_par::induce_sort8_par(text, len, suf, bkt.bounds, bkt.bounds + 1, left_most, threads);
+    else induce_sort8(text, len, suf, bkt, left_most);
+}
+
 /* src/psacak8.rs:19-53 psacak8. */
-void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr) {
+void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr, unsigned threads = 0) {
     if (len <= 3) {
         saca_tiny(text, len, suf);
         trace_push(tr, 0, 1, len, 0, 0, 0);
@@ -583,7 +598,7 @@ void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr) {
     Buckets bkt;
     bkt.build(text, len);
     put_lmscharacters8(text, len, suf, bkt);
-    induce_sort8(text, len, suf, bkt, true);
+    induce_sort8_any(text, len, suf, bkt, true, threads);
     size_t n = compact_left(suf, len, 0);
     size_t k = name_lmssubstrings(text, len, suf, n);
     uint32_t *suf1 = suf;
@@ -603,7 +618,7 @@ void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr) {
     }
     permutate_lmssuffixes(text, len, suf, n);
     put_lmssuffixes8(suf, len, bkt, n);
-    induce_sort8(text, len, suf, bkt, false);
+    induce_sort8_any(text, len, suf, bkt, false, threads);
 }
 
 /* src/psacak32.rs:912-943 translate_sample: ordered histogram, L -> bucket
@@ -680,6 +695,12 @@ int oracle_psacak32(const uint32_t *text, uint64_t n, uint32_t *sa, oracle_level
         saca_tiny(text, (size_t)n, sa);
     }
     if (n_levels) *n_levels = tr.count;
+    return 0;
+}
+
+int oracle_psacak8_par(const uint8_t *text, uint64_t n, uint32_t *sa, uint32_t threads) {
+    if (n >= 0xFFFFFFFFull) return -1;
+    psacak8_impl(text, (size_t)n, sa, nullptr, threads ? threads : 1);
     return 0;
 }
 

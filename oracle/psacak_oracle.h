@@ -46,6 +46,12 @@ int oracle_psacak8(const uint8_t *text, uint64_t n, uint32_t *sa,
 int oracle_psacak32(const uint32_t *text, uint64_t n, uint32_t *sa,
                     oracle_level *trace, uint32_t max_levels, uint32_t *n_levels);
 
+/* psacak8 with the reference's pipelined induced scans (src/pipeline.rs,
+ * src/psacak8.rs:201-344) on `threads` threads for texts of two blocks
+ * (2 x 128Ki) and more: the all-core CPU baseline.  Same result as
+ * oracle_psacak8.  Returns 0, or -1 when n >= 2^32-1. */
+int oracle_psacak8_par(const uint8_t *text, uint64_t n, uint32_t *sa, uint32_t threads);
+
 /* saca_tiny (src/common.rs:13-25): naive comparison sort of the suffixes. */
 void oracle_saca_tiny8(const uint8_t *text, uint64_t n, uint32_t *sa);
 void oracle_saca_tiny32(const uint32_t *text, uint64_t n, uint32_t *sa);

@@ -36,6 +36,7 @@ def lib():
         p, u64, u32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32
         _lib.oracle_psacak8.argtypes = [p, u64, p, p, u32, p]
         _lib.oracle_psacak32.argtypes = [p, u64, p, p, u32, p]
+        _lib.oracle_psacak8_par.argtypes = [p, u64, p, u32]
         _lib.oracle_saca_tiny8.argtypes = [p, u64, p]
         _lib.oracle_saca_tiny32.argtypes = [p, u64, p]
         _lib.oracle_translate_sample.argtypes = [p, u64, p]
@@ -66,6 +67,16 @@ def psacak8(text, trace=False):
     if rc != 0:
         raise ValueError("oracle_psacak8 rejected the input")
     return (sa, _levels(buf, min(cnt.value, 64))) if trace else sa
+
+
+def psacak8_par(text, threads):
+    """The reference's pipelined induced scans (fetch / induce / flush) on
+    `threads` threads; equal to psacak8."""
+    t = np.ascontiguousarray(np.frombuffer(bytes(text), dtype=np.uint8) if isinstance(text, (bytes, bytearray)) else text, dtype=np.uint8)
+    sa = np.zeros(t.size, dtype=np.uint32)
+    if lib().oracle_psacak8_par(_ptr(t), t.size, _ptr(sa), threads) != 0:
+        raise ValueError("oracle_psacak8_par rejected the input")
+    return sa
 
 
 def psacak32(text, trace=False):

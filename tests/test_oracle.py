@@ -125,3 +125,19 @@ def test_synthetic_traces_pinned():
             sa, tr = o.psacak8(t, trace=True)
         assert tr == case["levels"]
         assert o.hash_u32(sa) == case["sa_hash"]
+
+
+@pytest.mark.parametrize("threads", [1, 3, 8])
+def test_pipelined_scans_equal_serial(threads):
+    """The restatement of the reference's pipelined induced scans (the
+    all-core CPU baseline) builds the same suffix array as the serial
+    restatement: texts of several 128Ki blocks, with repeats, runs and an
+    all-equal stretch that sends writes far beyond the next block."""
+    from psacak_b200 import synth
+    rng = np.random.default_rng(threads)
+    texts = [synth.genome(3 << 20, seed=threads),
+             rng.integers(65, 69, 600_000).astype(np.uint8),
+             np.concatenate([np.full(300_000, 65, np.uint8), rng.integers(65, 70, 400_000).astype(np.uint8)]),
+             np.repeat(rng.integers(0, 256, 40_000).astype(np.uint8), rng.integers(1, 20, 40_000))]
+    for t in texts:
+        assert (o.psacak8_par(t, threads) == o.psacak8(t)).all()
