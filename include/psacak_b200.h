@@ -180,6 +180,30 @@ PSACAK_API int psacak_profile_get(psacak_ctx *ctx, psacak_kernel_stat *out, uint
 PSACAK_API int psacak_check_sa8_noalloc(const uint8_t *d_text, uint64_t n, const uint32_t *d_sa, int *ok,
                                         void *stream);
 
+/*
+ * Arrays derived from a suffix array `d_sa` of n entries (sentinel excluded,
+ * as psacak8 / psacak32 produce it), on the device.  hucsmn/psacak has no
+ * counterpart; these are the usual consumers of its output.  All pointers
+ * are device pointers except `primary`; work is ordered on `stream` (NULL =
+ * the context's stream) and the call returns when it has finished.
+ *
+ * psacak_isa_dev: inverse suffix array, d_isa[d_sa[i]] = i.
+ * psacak_bwt8_dev: Burrows-Wheeler transform of text + sentinel without the
+ *   sentinel character (libdivsufsort's divbwt convention): d_bwt[0] =
+ *   text[n-1], then text[SA[i]-1] for every i with SA[i] > 0 in SA order;
+ *   *primary = 1 + the i with SA[i] = 0 (the sentinel's row).  n bytes out.
+ * psacak_lcp8_dev / psacak_lcp32_dev: LCP array, d_lcp[0] = 0 and d_lcp[i]
+ *   = length of the longest common prefix of the suffixes SA[i-1] and
+ *   SA[i].  Work O(n log n) for any text (permuted-LCP method).
+ */
+PSACAK_API int psacak_isa_dev(psacak_ctx *ctx, const uint32_t *d_sa, uint64_t n, uint32_t *d_isa, void *stream);
+PSACAK_API int psacak_bwt8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, const uint32_t *d_sa,
+                               uint8_t *d_bwt, uint64_t *primary, void *stream);
+PSACAK_API int psacak_lcp8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, const uint32_t *d_sa,
+                               uint32_t *d_lcp, void *stream);
+PSACAK_API int psacak_lcp32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, const uint32_t *d_sa,
+                                uint32_t *d_lcp, void *stream);
+
 /* Number of kernels the library launched since the context was created. */
 PSACAK_API uint64_t psacak_kernel_launches(psacak_ctx *ctx);
 

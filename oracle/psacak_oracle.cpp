@@ -665,6 +665,29 @@ int check_sa(const C *text, uint64_t n, const uint32_t *sa) {
 
 }  // namespace
 
+/* LCP array by Kasai, Lee, Arimura, Arikawa, Park (CPM 2001): inverse
+ * suffix array, then the LCP of each suffix with its predecessor in text
+ * order, each start one below the previous value.  lcp[0] = 0. */
+template <class C>
+void kasai(const C *text, uint64_t n, const uint32_t *sa, uint32_t *lcp) {
+    if (n == 0) return;
+    std::vector<uint32_t> rank(n);
+    for (uint64_t i = 0; i < n; i++) rank[sa[i]] = (uint32_t)i;
+    uint64_t h = 0;
+    lcp[0] = 0;
+    for (uint64_t j = 0; j < n; j++) {
+        if (rank[j] == 0) {
+            h = 0;
+            continue;
+        }
+        uint64_t k = sa[rank[j] - 1];
+        while (j + h < n && k + h < n && text[j + h] == text[k + h]) h++;
+        lcp[rank[j]] = (uint32_t)h;
+        if (h > 0) h--;
+    }
+}
+
+
 extern "C" {
 
 uint64_t oracle_hash_u32(const uint32_t *v, uint64_t n) {
@@ -725,6 +748,24 @@ int oracle_check_sa8(const uint8_t *text, uint64_t n, const uint32_t *sa) {
 
 int oracle_check_sa32(const uint32_t *text, uint64_t n, const uint32_t *sa) {
     return check_sa(text, n, sa);
+}
+
+void oracle_lcp8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint32_t *lcp) { kasai(text, n, sa, lcp); }
+void oracle_lcp32(const uint32_t *text, uint64_t n, const uint32_t *sa, uint32_t *lcp) { kasai(text, n, sa, lcp); }
+
+/* Burrows-Wheeler transform of text + sentinel, the sentinel's character
+ * left out (libdivsufsort's divbwt convention): bwt[0] = text[n-1], then
+ * text[sa[i]-1] in suffix order skipping sa[i] = 0, whose row (i + 1) is
+ * returned as the primary index. */
+uint64_t oracle_bwt8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint8_t *bwt) {
+    if (n == 0) return 0;
+    uint64_t primary = 0, o = 1;
+    bwt[0] = text[n - 1];
+    for (uint64_t i = 0; i < n; i++) {
+        if (sa[i] == 0) primary = i + 1;
+        else bwt[o++] = text[sa[i] - 1];
+    }
+    return primary;
 }
 
 uint64_t oracle_reduced8(const uint8_t *text, uint64_t n, uint32_t *out, uint64_t cap,

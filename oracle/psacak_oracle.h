@@ -52,6 +52,13 @@ int oracle_psacak32(const uint32_t *text, uint64_t n, uint32_t *sa,
  * oracle_psacak8.  Returns 0, or -1 when n >= 2^32-1. */
 int oracle_psacak8_par(const uint8_t *text, uint64_t n, uint32_t *sa, uint32_t threads);
 
+/* Derived arrays (no counterpart in the reference): LCP by Kasai et al.
+ * (lcp[0] = 0), BWT in libdivsufsort's divbwt convention (returns the
+ * primary index; bwt has n bytes). */
+void oracle_lcp8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint32_t *lcp);
+void oracle_lcp32(const uint32_t *text, uint64_t n, const uint32_t *sa, uint32_t *lcp);
+uint64_t oracle_bwt8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint8_t *bwt);
+
 /* saca_tiny (src/common.rs:13-25): naive comparison sort of the suffixes. */
 void oracle_saca_tiny8(const uint8_t *text, uint64_t n, uint32_t *sa);
 void oracle_saca_tiny32(const uint32_t *text, uint64_t n, uint32_t *sa);

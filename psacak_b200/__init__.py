@@ -128,6 +128,12 @@ def lib():
         L.psacak_check_sa8_noalloc.restype = i32
         L.psacak_kernel_launches.argtypes = [p]
         L.psacak_kernel_launches.restype = u64
+        L.psacak_isa_dev.argtypes = [p, p, u64, p, p]
+        L.psacak_bwt8_dev.argtypes = [p, p, u64, p, p, ctypes.POINTER(u64), p]
+        L.psacak_lcp8_dev.argtypes = [p, p, u64, p, p, p]
+        L.psacak_lcp32_dev.argtypes = [p, p, u64, p, p, p]
+        for f in (L.psacak_isa_dev, L.psacak_bwt8_dev, L.psacak_lcp8_dev, L.psacak_lcp32_dev):
+            f.restype = i32
         for name in ("psacak8", "psacak32", "psacak8_ctx", "psacak32_ctx", "psacak8_dev", "psacak32_dev",
                      "psacak8_batch", "psacak_get_trace", "psacak_check_sa8_dev", "psacak_check_sa32_dev",
                      "psacak_ctx_create", "psacak_ctx_destroy", "psacak_profile_enable", "psacak_profile_reset",
@@ -228,6 +234,29 @@ class Context:
         off = np.ascontiguousarray(offsets, dtype=np.uint64)
         _raise(lib().psacak8_batch_dev(self._h, ctypes.c_void_p(d_texts), _vp(off), off.size - 1,
                                        ctypes.c_void_p(d_sas), ctypes.c_void_p(stream), _sched_ptr(schedule)))
+
+    def isa_dev(self, d_sa, n, d_isa, stream=0):
+        """Inverse suffix array: d_isa[d_sa[i]] = i (device pointers)."""
+        _raise(lib().psacak_isa_dev(self._h, ctypes.c_void_p(d_sa), n, ctypes.c_void_p(d_isa),
+                                    ctypes.c_void_p(stream)))
+
+    def bwt8_dev(self, d_text, n, d_sa, d_bwt, stream=0):
+        """BWT of text + sentinel without the sentinel character (divbwt
+        convention) into d_bwt (n bytes); returns the primary index."""
+        primary = ctypes.c_uint64(0)
+        _raise(lib().psacak_bwt8_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                     ctypes.c_void_p(d_bwt), ctypes.byref(primary), ctypes.c_void_p(stream)))
+        return int(primary.value)
+
+    def lcp8_dev(self, d_text, n, d_sa, d_lcp, stream=0):
+        """LCP array of a byte text and its suffix array (device pointers)."""
+        _raise(lib().psacak_lcp8_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                     ctypes.c_void_p(d_lcp), ctypes.c_void_p(stream)))
+
+    def lcp32_dev(self, d_text, n, d_sa, d_lcp, stream=0):
+        """LCP array of a u32 text and its suffix array (device pointers)."""
+        _raise(lib().psacak_lcp32_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
+                                      ctypes.c_void_p(d_lcp), ctypes.c_void_p(stream)))
 
     def check_sa8_dev(self, d_text, n, d_sa, stream=0):
         ok = ctypes.c_int(0)

@@ -37,6 +37,10 @@ def lib():
         _lib.oracle_psacak8.argtypes = [p, u64, p, p, u32, p]
         _lib.oracle_psacak32.argtypes = [p, u64, p, p, u32, p]
         _lib.oracle_psacak8_par.argtypes = [p, u64, p, u32]
+        _lib.oracle_lcp8.argtypes = [p, u64, p, p]
+        _lib.oracle_lcp32.argtypes = [p, u64, p, p]
+        _lib.oracle_bwt8.argtypes = [p, u64, p, p]
+        _lib.oracle_bwt8.restype = u64
         _lib.oracle_saca_tiny8.argtypes = [p, u64, p]
         _lib.oracle_saca_tiny32.argtypes = [p, u64, p]
         _lib.oracle_translate_sample.argtypes = [p, u64, p]
@@ -77,6 +81,28 @@ def psacak8_par(text, threads):
     if lib().oracle_psacak8_par(_ptr(t), t.size, _ptr(sa), threads) != 0:
         raise ValueError("oracle_psacak8_par rejected the input")
     return sa
+
+
+def lcp(text, sa):
+    """LCP array (Kasai et al.) of `text` (u8 or u32) with suffix array `sa`."""
+    t = np.ascontiguousarray(text)
+    s = np.ascontiguousarray(sa, dtype=np.uint32)
+    out = np.zeros(s.size, dtype=np.uint32)
+    if t.dtype == np.uint8:
+        lib().oracle_lcp8(_ptr(t), t.size, _ptr(s), _ptr(out))
+    else:
+        t = np.ascontiguousarray(t, dtype=np.uint32)
+        lib().oracle_lcp32(_ptr(t), t.size, _ptr(s), _ptr(out))
+    return out
+
+
+def bwt(text, sa):
+    """(BWT bytes, primary index) in libdivsufsort's divbwt convention."""
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    s = np.ascontiguousarray(sa, dtype=np.uint32)
+    out = np.zeros(t.size, dtype=np.uint8)
+    primary = lib().oracle_bwt8(_ptr(t), t.size, _ptr(s), _ptr(out))
+    return out, int(primary)
 
 
 def psacak32(text, trace=False):

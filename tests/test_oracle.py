@@ -141,3 +141,38 @@ def test_pipelined_scans_equal_serial(threads):
              np.repeat(rng.integers(0, 256, 40_000).astype(np.uint8), rng.integers(1, 20, 40_000))]
     for t in texts:
         assert (o.psacak8_par(t, threads) == o.psacak8(t)).all()
+
+
+def _naive_lcp(t, sa):
+    out = [0] * len(sa)
+    for i in range(1, len(sa)):
+        a, b, h = int(sa[i - 1]), int(sa[i]), 0
+        while a + h < len(t) and b + h < len(t) and t[a + h] == t[b + h]:
+            h += 1
+        out[i] = h
+    return out
+
+
+def test_lcp_and_bwt_restatements_match_definitions():
+    """Kasai's LCP and the divbwt-convention BWT of the oracle against their
+    definitions: direct suffix comparison, and the sorted rotations of
+    text + sentinel with the sentinel's character left out."""
+    rng = np.random.default_rng(11)
+    cases = [b"mississippi", b"a", b"aaaa", b"abab", b"banana"] + [
+        bytes(rng.integers(97, 97 + int(rng.integers(1, 5)), int(rng.integers(1, 60))).astype(np.uint8))
+        for _ in range(300)]
+    for t in cases:
+        a = np.frombuffer(t, np.uint8)
+        sa = o.psacak8(a)
+        assert o.lcp(a, sa).tolist() == _naive_lcp(t, sa), t
+        # rotations of t + sentinel (sentinel below every byte), sorted
+        u = list(t) + [-1]
+        rot = sorted(range(len(u)), key=lambda r: u[r:] + u[:r])
+        full = [u[r - 1] for r in rot]
+        primary = full.index(-1)
+        want = [c for c in full if c != -1]
+        got, p = o.bwt(a, sa)
+        assert got.tolist() == want and p == primary, t
+    u32 = rng.integers(0, 7, 500).astype(np.uint32)
+    sa = o.psacak32(u32)
+    assert o.lcp(u32, sa).tolist() == _naive_lcp(u32.tolist(), sa)
