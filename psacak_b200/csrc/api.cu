@@ -58,6 +58,28 @@ __global__ void k_count_s(const uint32_t *__restrict__ text, uint64_t n, const u
     }
 }
 
+// Byte text as u32 bucket ids, with the byte histogram in heads[0..256).
+__global__ void k_byte_names(const uint8_t *__restrict__ text, uint64_t n, uint32_t *names, uint32_t *heads) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t c = text[i];
+        names[i] = c;
+        atomicAdd(&h[c], 1u);
+    }
+    __syncthreads();
+    if (h[threadIdx.x]) atomicAdd(&heads[threadIdx.x], h[threadIdx.x]);
+}
+// Counts in heads[0..256) -> bucket heads (exclusive prefix), heads[256] = n.
+__global__ void k_byte_heads(uint32_t *heads, uint32_t n) {
+    __shared__ uint32_t s_scan[33];
+    uint32_t ex;
+    block_scan<uint32_t, OpSum<uint32_t>, 256>(heads[threadIdx.x], OpSum<uint32_t>(), s_scan, &ex, (uint32_t *)nullptr);
+    heads[threadIdx.x] = ex;
+    if (threadIdx.x == 0) heads[256] = n;
+}
+
 struct SortedLmsPred {
     const uint32_t *sa;
     const uint32_t *lms;
@@ -136,6 +158,21 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         if (names && bheads && ctx.sched.finish_below && n < ctx.sched.finish_below) {
             trace_push(ctx, level, width, n, 0, 0, 0);
             return sort_by_doubling(ctx, names, bheads, nbuckets, n, sa, s);
+        }
+    } else {
+        // the same for a short byte text: the bytes are the bucket ids
+        if (ctx.sched.finish_below && n < ctx.sched.finish_below) {
+            DBuf<uint32_t> bnames, bh;
+            PSK_TRY(bnames.init(ctx, n));
+            PSK_TRY(bh.init(ctx, 257));
+            PSK_CUDA(cudaMemsetAsync(bh.get(), 0, 257 * sizeof(uint32_t), s));
+            k_byte_names<<<grid_for(n, 4096), 256, 0, s>>>(text, n, bnames, bh);
+            PSK_KCOUNT();
+            k_byte_heads<<<1, 256, 0, s>>>(bh, (uint32_t)n);
+            PSK_KCOUNT();
+            PSK_LAUNCH_CHECK();
+            trace_push(ctx, level, width, n, 0, 0, 0);
+            return sort_by_doubling(ctx, bnames, bh, 256, n, sa, s);
         }
     }
     const uint64_t nwords = ceil_div(n, 32);

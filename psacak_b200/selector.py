@@ -1,7 +1,9 @@
 """Learned schedule selection for psacak_b200.
 
 * ``SCHEDULES`` -- the candidate schedules (engine of the byte level x scatter
-  tile size x recursion strategy).  Every one builds the same suffix array.
+  tile size x recursion strategy: levels shorter than ``finish_below`` --
+  level 0 included -- are sorted directly by prefix doubling).  Every one
+  builds the same suffix array.
 * ``features`` -- 16 text statistics computed on the GPU (psacak_text_stats).
 * ``autotune`` -- exhaustive search: times every schedule on a text.  It is
   the fallback when no trained model is available and the judge of the
@@ -24,7 +26,7 @@ NH = 64
 
 SCHEDULES = [
     {"engine": e, "inner_engine": ENGINE_DOUBLING, "tile_items": t, "finish_below": f}
-    for e in (ENGINE_BUCKET, ENGINE_DOUBLING) for t in (8, 12, 16) for f in (0, 1 << 16)
+    for e in (ENGINE_BUCKET, ENGINE_DOUBLING) for t in (8, 12, 16) for f in (0, 1 << 16, 1 << 20, 1 << 24)
 ]
 DEFAULT_INDEX = SCHEDULES.index({"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 8,
                                  "finish_below": 0})

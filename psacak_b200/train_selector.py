@@ -3,10 +3,12 @@
     python -m psacak_b200.train_selector --texts 160 --out psacak_b200/models/selector.npz
 
 Training texts follow the serving mix (lengths log-uniform on [4 KiB, 64 MiB]
-symbols, half u8 ACGT, half u32 over 2^16, generated on the device); each is
-autotuned exhaustively (every schedule timed with CUDA events), the
-statistics kernel gives its features, and the MLP is fitted to log2(ms) on
-the GPU.  A held-out quarter measures regret against the exhaustive best,
+symbols, half u8 ACGT, half u32 over 2^16, generated on the device), plus a
+quarter as many genome-like u8 texts (order-3 Markov with N runs and long
+mutated copies, 64 KiB .. 64 MiB) so that the model sees what long repeats
+cost the prefix-doubling schedules; each is autotuned exhaustively (every
+schedule timed with CUDA events), the statistics kernel gives its features,
+and the MLP is fitted to log2(ms) on the GPU.  A held-out quarter measures regret against the exhaustive best,
 beside the fixed default schedule; the report is printed as JSON and saved
 next to the model.
 """
@@ -33,16 +35,23 @@ def main(argv=None):
     from psacak_b200 import selector as sel
     from psacak_b200 import serve
 
+    from psacak_b200 import synth
     ctx = pk.Context(0)
     plan = serve.request_plan(args.texts, args.seed)
-    maxn = max(n for n, _, _ in plan)
+    genome = [(int(m), 0, args.seed + 1000 + i)
+              for i, m in enumerate(synth.loguniform(args.texts // 4, 64 << 10, 64 << 20, args.seed + 1))]
+    maxn = max(n for n, _, _ in plan + genome)
     d_text = torch.empty(maxn * 4, dtype=torch.uint8, device="cuda")
     d_sa = torch.empty(maxn, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
     X, T = [], []
     t0 = time.perf_counter()
-    for i, (n, w, s) in enumerate(plan):
-        serve.make_text(ctx, d_text.data_ptr(), n, w, s, stream.cuda_stream)
+    for i, (n, w, s) in enumerate(plan + genome):
+        if w == 0:  # genome-like bytes, generated on the host
+            w = 1
+            d_text[:n].copy_(torch.from_numpy(synth.genome(n, seed=s)))
+        else:
+            serve.make_text(ctx, d_text.data_ptr(), n, w, s, stream.cuda_stream)
         torch.cuda.synchronize()
         X.append(sel.features(ctx, d_text.data_ptr(), n, w))
         T.append(sel.autotune(ctx, d_text.data_ptr(), n, w, d_sa.data_ptr(), reps=2))

@@ -144,3 +144,16 @@ def test_every_schedule_gives_the_same_sa(ctx):
     want = o.psacak32(sym)
     for sc in SCHEDULES:
         assert (ctx.psacak32(sym, sc) == want).all(), sc
+
+
+@pytest.mark.parametrize("finish", [1 << 12, 1 << 16, 1 << 22])
+def test_byte_texts_sorted_directly_by_prefix_doubling(ctx, finish):
+    """Byte texts shorter than finish_below skip the induced scans and are
+    sorted by prefix doubling from their bytes; the SA is the same."""
+    rng = np.random.default_rng(finish)
+    texts = [np.frombuffer(b"mississippi", np.uint8), np.frombuffer(b"aaaa", np.uint8),
+             rng.integers(65, 69, 3000).astype(np.uint8), synth.genome(40_000, seed=3),
+             np.full(5000, 0, np.uint8), rng.integers(0, 256, 60_000).astype(np.uint8)]
+    for t in texts:
+        sc = {"engine": pk.ENGINE_BUCKET, "inner_engine": pk.ENGINE_DOUBLING, "finish_below": finish}
+        assert (ctx.psacak(t, sc) == o.psacak8(t)).all(), (finish, t.size)
