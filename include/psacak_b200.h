@@ -39,16 +39,20 @@ extern "C" {
 #define PSACAK_ENGINE_BUCKET 1   /* bucket-ordered scan (alphabets <= 256 only) */
 #define PSACAK_ENGINE_DOUBLING 2 /* chain-doubling scan (any alphabet) */
 
-/* Tunables of one build.  Zero fields mean "use the default".  Every
- * schedule gives the same suffix array; it only changes speed. */
+/* Tunables of one build.  Zero fields mean "use the default" (finish_below:
+ * 0 = never).  A NULL schedule is the zero schedule with finish_below =
+ * PSACAK_DEFAULT_FINISH_BELOW.  Every schedule gives the same suffix array;
+ * it only changes speed. */
+#define PSACAK_DEFAULT_FINISH_BELOW (1u << 16)
 typedef struct {
     uint32_t engine;           /* PSACAK_ENGINE_* for level 0 */
     uint32_t inner_engine;     /* PSACAK_ENGINE_* for levels >= 1 */
-    uint32_t scan_ctas_per_sm; /* CTAs per SM of the chunked scans (0 = 4) */
+    uint32_t scan_ctas_per_sm; /* CTAs per SM of the grid-stride helper kernels (0 = 4) */
     uint32_t batch_chunk_mib;  /* batch builds: max MiB per concatenated build (0 = 3072) */
     uint32_t tile_items;       /* items per thread of the bucket scatter and compactions: 8, 12 or 16 (0 = 8) */
-    uint32_t finish_below;     /* recursion strategy: integer levels shorter than this are sorted
-                                  directly by prefix doubling instead of recursing (0 = never) */
+    uint32_t finish_below;     /* recursion strategy: levels shorter than this (the text itself
+                                  included) are sorted directly by prefix doubling instead of
+                                  induced sorting and recursion (0 = never) */
     uint32_t reserved[2];
 } psacak_schedule;
 

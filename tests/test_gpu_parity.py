@@ -102,7 +102,7 @@ def test_synthetic_traces(ctx, engine):
     for case in load("synthetic_traces.json"):
         t = make_input(case["generator"], case["n"], case["seed"])
         if case["generator"] == "zipf32":
-            sa = ctx.psacak32(t)
+            sa = ctx.psacak32(t, {})  # explicit zero schedule: recursion all the way down, as the oracle's trace
         else:
             sa = ctx.psacak(t, sched(engine))
         assert o.hash_u32(sa) == case["sa_hash"], case["name"]
