@@ -270,7 +270,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
 
     // Stage 2: name them and build the reduced string.
     DBuf<uint32_t> red, heads, flags, sa1, names1;
-    DBuf<uint64_t> sorted_pc;  // byte levels, bucket engine: final-mode LMS list with predecessor characters
+    DBuf<uint64_t> sorted_win;  // byte levels, bucket engine: final-mode LMS list with predecessor windows
     uint32_t k = 0;
     if (n1 > 0 && !extracted) {
         PSK_TRY(ctx.compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_scalars + 1,
@@ -338,17 +338,17 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         }
         if constexpr (sizeof(C) == 1) {
             if (engine == PSACAK_ENGINE_BUCKET) {
-                // the bucket scans take the list with predecessor characters
+                // the bucket scans take the list with predecessor windows
                 red.reset();
                 names1.reset();
                 DBuf<uint64_t> plist;
-                PSK_TRY(sorted_pc.init(ctx, n1));
+                PSK_TRY(sorted_win.init(ctx, n1));
                 PSK_TRY(plist.init(ctx, n1));
-                PSK_TRY(permute_lms8(sa1, n1, text, lms, pref, n, plist, sorted_pc, ctx.d_err, s));
+                PSK_TRY(permute_lms8(sa1, n1, text, lms, pref, n, plist, sorted_win, ctx.d_err, s));
             }
         }
         // red is free again; reuse it as the position list of the permutation.
-        if (!sorted_pc.get()) PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
+        if (!sorted_win.get()) PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
     } else {
         if (level == 0 && ctx.debug_red) {
             ctx.debug_n1 = 0;
@@ -365,7 +365,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     if constexpr (sizeof(C) == 1) {
         if (engine == PSACAK_ENGINE_BUCKET) {
             sa1.reset();
-            return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sorted_pc, n1, sa, s);
+            return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sorted_win, n1, sa, s);
         }
         return induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
     } else {
@@ -596,7 +596,7 @@ struct ProfGuard {
 
 // Folds the device-side count of entries scattered by the bucket scans into
 // the "induce_scatter" class (per entry: the entry and its predecessor
-// character written, 5 bytes, and one text byte read in front of it).
+// window written, 8 bytes, and one text byte read in front of it).
 static status_t profile_collect(Ctx &c) {
     if (!c.profiling) return PSACAK_OK;
     c.prof.resolve();
@@ -606,7 +606,7 @@ static status_t profile_collect(Ctx &c) {
     unsigned long long induced = ((unsigned long long)h[1] << 32) | h[0];
     if (induced) {
         int cls = c.prof.cls_of("induce_scatter");
-        c.prof.stats[cls].bytes += 6ull * induced;
+        c.prof.stats[cls].bytes += 9ull * induced;
     }
     return PSACAK_OK;
 }

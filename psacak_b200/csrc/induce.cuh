@@ -76,10 +76,10 @@ status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bhead
 // then scattered to the higher buckets in scan order; the S scan mirrors it.
 // In INDUCE_LMS_SUBSTRINGS mode with `lms_out` set, the S scan also writes the
 // n1 LMS positions in sorted-substring order to lms_out.
-// In INDUCE_FINAL mode `sorted_pc` lists the sorted LMS suffixes as
-// (position << 8) | predecessor character.
+// In INDUCE_FINAL mode `sorted_win` lists the sorted LMS suffixes as
+// position | predecessor window << 32 (win_fill).
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms,
-                        const ByteGeom &hgeom, const ByteGeom *dgeom, InduceMode mode, const uint64_t *sorted_pc,
+                        const ByteGeom &hgeom, const ByteGeom *dgeom, InduceMode mode, const uint64_t *sorted_win,
                         uint64_t n1, uint32_t *sa, cudaStream_t s, uint32_t *lms_out = nullptr);
 
 }  // namespace psk

@@ -63,7 +63,7 @@ constexpr int PL_UNROLL = 4;
 __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__restrict__ text, uint64_t nwords,
                                                              const uint32_t *__restrict__ lms,
                                                              const ByteGeom *__restrict__ g, uint32_t *cursor,
-                                                             uint32_t *sa, uint8_t *c0s, uint64_t wchunk) {
+                                                             uint32_t *sa, uint32_t *wins, uint64_t wchunk) {
     __shared__ uint32_t s_cnt[256], s_base[256], s_tail[256];
     s_cnt[threadIdx.x] = 0;
     s_tail[threadIdx.x] = g->tail[threadIdx.x];
@@ -73,8 +73,7 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
     const uint64_t w1 = w0 + wchunk < nwords ? w0 + wchunk : nwords;
     for (int pass = 0; pass < 2; pass++) {
         for (uint64_t wb = w0 + warp; wb < w1; wb += PL_WARPS * PL_UNROLL) {
-            uint32_t word[PL_UNROLL], c[PL_UNROLL];
-            uint8_t pc[PL_UNROLL];
+            uint32_t word[PL_UNROLL], c[PL_UNROLL], pw[PL_UNROLL];
 #pragma unroll
             for (int u = 0; u < PL_UNROLL; u++) {
                 const uint64_t w = wb + (uint64_t)u * PL_WARPS;
@@ -85,7 +84,7 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
                 const uint64_t p = ((wb + (uint64_t)u * PL_WARPS) << 5) + lane;  // LMS positions are > 0
                 const bool on = (word[u] >> lane) & 1u;
                 c[u] = on ? text[p] : 256u;
-                pc[u] = (pass == 1 && on) ? text[p - 1] : 0;
+                pw[u] = (pass == 1 && on) ? win_fill(text, (uint32_t)p) : 0u;
             }
 #pragma unroll
             for (int u = 0; u < PL_UNROLL; u++) {
@@ -100,7 +99,7 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
                 if (pass == 1 && on) {
                     const uint32_t slot = s_tail[cc] - 1 - (s_base[cc] + got + __popc(peers & lt));
                     sa[slot] = (uint32_t)(((wb + (uint64_t)u * PL_WARPS) << 5) + lane);
-                    c0s[slot] = pc[u];
+                    wins[slot] = pw[u];
                 }
             }
         }
@@ -115,12 +114,12 @@ __global__ void __launch_bounds__(PL_BLOCK) k_place_lms_any8(const uint8_t *__re
 }
 
 // Final mode placement: the sorted LMS suffixes fill the tail of each
-// bucket in order.  Entry i of the list is (position << 8 | predecessor
-// character); its bucket is the one whose LMS range holds i (a binary
+// bucket in order.  Entry i of the list is position | predecessor window
+// << 32; its bucket is the one whose LMS range holds i (a binary
 // search over the 256 ranges in shared memory), so the text is not read.
 __global__ void __launch_bounds__(256) k_place_lms_sorted8(const uint64_t *__restrict__ sorted, uint64_t n1,
                                                            const ByteGeom *__restrict__ g, uint32_t *sa,
-                                                           uint8_t *c0s) {
+                                                           uint32_t *wins) {
     __shared__ uint32_t s_start[256], s_off[256];  // slot of list entry i = s_off[c] + i
     s_start[threadIdx.x] = g->lmsstart[threadIdx.x];
     s_off[threadIdx.x] = g->tail[threadIdx.x] - g->lmscount[threadIdx.x] - g->lmsstart[threadIdx.x];
@@ -133,22 +132,22 @@ __global__ void __launch_bounds__(256) k_place_lms_sorted8(const uint64_t *__res
         for (uint32_t step = 128; step > 0; step >>= 1)
             if (s_start[c + step] <= (uint32_t)i) c += step;
         const uint32_t slot = s_off[c] + (uint32_t)i;
-        sa[slot] = (uint32_t)(v >> 8);
-        c0s[slot] = (uint8_t)v;
+        sa[slot] = (uint32_t)v;
+        wins[slot] = (uint32_t)(v >> 32);
     }
 }
 
 // cursors: L scan starts at the bucket heads, S scan at the tails; the
 // sentinel suffix n-1 is the first entry of its bucket (src/psacak8.rs:131-135).
 __global__ void k_init_cursors(const ByteGeom *__restrict__ g, const uint8_t *__restrict__ text, uint64_t n,
-                               uint32_t *curL, uint32_t *curS, uint32_t *sa, uint8_t *c0s) {
+                               uint32_t *curL, uint32_t *curS, uint32_t *sa, uint32_t *wins) {
     int c = threadIdx.x;
     uint8_t last = text[n - 1];
     curL[c] = g->head[c] + (c == last ? 1u : 0u);
     curS[c] = g->tail[c];
     if (c == 0) {
         sa[g->head[last]] = (uint32_t)(n - 1);
-        c0s[g->head[last]] = n >= 2 ? text[n - 2] : 0;
+        wins[g->head[last]] = n >= 2 ? win_fill(text, (uint32_t)(n - 1)) : 0u;
     }
 }
 
@@ -160,7 +159,7 @@ __global__ void k_init_cursors(const ByteGeom *__restrict__ g, const uint8_t *__
 // C_d = #{q : runs[q] >= d}.
 //
 // Step 1, one look-back scan over the seeds: the load measures each seed's
-// run (the characters c in front of it; c0s already holds the first), the
+// run (the characters c in front of it; its window holds the first three), the
 // scan counts runs >= 1 and >= 2, and the store places every depth-1 cell and
 // lists the seeds with runs >= 2 as a sub-problem: seed x - 1 with run r - 1,
 // whose cells are exactly the original depths 2, 3, ...  Step 2 solves the
@@ -199,7 +198,7 @@ struct SeedLoad {
     static constexpr int kIPT = 8;
     const uint8_t *text;
     const uint32_t *sa;
-    const uint8_t *c0s;
+    const uint32_t *wins;
     uint32_t start;
     int dir;
     uint8_t c;
@@ -209,13 +208,20 @@ struct SeedLoad {
         uint32_t r = 0;
         uint8_t b = 0;
         if (x > 0) {
-            b = c0s[slot];
+            const uint32_t w = wins[slot];
+            b = (uint8_t)w;
             if (b == c) {
-                // measured up to CHAIN_CAP characters here; a longer run is
-                // finished by k_chain_totals over the sub-list, so that no
-                // tile waits on a long run (the next tiles' look-back would)
+                // measured up to CHAIN_CAP characters here (the window's
+                // look-ahead bytes first); a longer run is finished by
+                // k_chain_totals over the sub-list, so that no tile waits on
+                // a long run (the next tiles' look-back would)
+                const uint32_t ahead = w >> 24;
                 r = 1;
-                while (r < x && r < CHAIN_CAP && (b = text[x - r - 1]) == c) r++;
+                while (r < x && r < CHAIN_CAP) {
+                    b = r <= ahead ? (uint8_t)(w >> (8 * r)) : text[x - r - 1];
+                    if (b != c) break;
+                    r++;
+                }
                 if (r == x) b = 0;
                 else if (r == CHAIN_CAP && b == c) r |= CHAIN_LONG;
             }
@@ -229,7 +235,7 @@ struct SeedLoad {
 };
 struct SeedStore {
     uint32_t *sa;
-    uint8_t *c0s;
+    uint32_t *wins;
     uint32_t *subx, *subr;
     uint8_t *sube;
     uint32_t first, limit;  // slot of the first cell; C_1
@@ -245,7 +251,7 @@ struct SeedStore {
         }
         const uint32_t slot = dir > 0 ? first + ex.c1 : first - ex.c1;
         sa[slot] = p.x - 1;
-        c0s[slot] = r > 1 ? c : p.e;
+        wins[slot] = run_win(1, r, c, p.e);
         if (r >= 2) {
             subx[ex.c2] = p.x - 1;
             subr[ex.c2] = (r - 1) | (p.r & CHAIN_LONG);  // a long run's length is finished later
@@ -332,8 +338,8 @@ __global__ void __launch_bounds__(256) k_chain_totals(const uint8_t *__restrict_
 }
 
 // Sub-list scan: per seed its ChainCounts; the store writes the seed's cells
-// of depth 1..3 (entry and predecessor character) and the offset of its
-// deep cells.
+// of depth 1..3 (entry and predecessor window) and the offset of its deep
+// cells.
 struct ChainLoad {
     using Payload = ChainPayload;
     static constexpr int kIPT = 6;
@@ -349,7 +355,7 @@ struct ChainLoad {
 };
 struct ChainStore {
     uint32_t *sa;
-    uint8_t *c0s;
+    uint32_t *wins;
     uint32_t *deep_off;  // null when the sub-list has no deep cells
     uint32_t first;      // slot of the first cell
     uint32_t base2, base3;  // C_1 and C_1 + C_2
@@ -357,26 +363,26 @@ struct ChainStore {
     int dir;
     uint8_t c;
     uint32_t *err;
-    __device__ __forceinline__ void put(uint32_t k, uint32_t val, uint8_t pc) const {
+    __device__ __forceinline__ void put(uint32_t k, uint32_t val, uint32_t w) const {
         if (k >= limit) {
             dev_fail(err, DEVERR_RANGE);
             return;
         }
         const uint32_t slot = dir > 0 ? first + k : first - k;
         sa[slot] = val;
-        c0s[slot] = pc;
+        wins[slot] = w;
     }
     __device__ __forceinline__ void operator()(uint64_t q, ChainCounts ex, ChainCounts, const ChainPayload &p) const {
         const uint32_t r = p.r;
-        if (r >= 1) put(ex.c1, p.x - 1, r > 1 ? c : p.e);
-        if (r >= 2) put(base2 + ex.c2, p.x - 2, r > 2 ? c : p.e);
-        if (r >= 3) put(base3 + ex.c3, p.x - 3, r > 3 ? c : p.e);
+        if (r >= 1) put(ex.c1, p.x - 1, run_win(1, r, c, p.e));
+        if (r >= 2) put(base2 + ex.c2, p.x - 2, run_win(2, r, c, p.e));
+        if (r >= 3) put(base3 + ex.c3, p.x - 3, run_win(3, r, c, p.e));
         if (deep_off) deep_off[q] = ex.deep;
     }
 };
 
 // Deep cell q (row-major over sub-list seeds, depths > 3) -> (depth - 3,
-// value (seed - depth) << 8 | the character in front of that suffix).
+// value (seed - depth) | the window of that suffix << 32).
 __global__ void k_expand_deep(const uint32_t *__restrict__ xs, uint32_t nseeds, const uint32_t *__restrict__ off,
                               const uint32_t *__restrict__ runs, const uint8_t *__restrict__ endc, uint8_t c,
                               uint32_t ncells, uint32_t *keys, uint64_t *vals) {
@@ -391,19 +397,18 @@ __global__ void k_expand_deep(const uint32_t *__restrict__ xs, uint32_t nseeds, 
         uint32_t dd = q - off[lo] + 1;
         uint32_t d = dd + CHAIN_DIRECT;
         uint32_t x = xs[lo];
-        uint8_t pc = d < runs[lo] ? c : endc[lo];
         keys[q] = dd;
-        vals[q] = ((uint64_t)(x - d) << 8) | pc;
+        vals[q] = (uint64_t)(x - d) | (uint64_t)run_win(d, runs[lo], c, endc[lo]) << 32;
     }
 }
 
 __global__ void k_place_cells(const uint64_t *__restrict__ vals, uint32_t ncells, uint32_t first, int dir,
-                              uint32_t *sa, uint8_t *c0s) {
+                              uint32_t *sa, uint32_t *wins) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ncells; q += gridDim.x * blockDim.x) {
         uint32_t slot = dir > 0 ? first + q : first - q;
         uint64_t v = vals[q];
-        sa[slot] = (uint32_t)(v >> 8);
-        c0s[slot] = (uint8_t)v;
+        sa[slot] = (uint32_t)v;
+        wins[slot] = (uint32_t)(v >> 32);
     }
 }
 
@@ -423,10 +428,10 @@ __global__ void k_place_cells(const uint64_t *__restrict__ vals, uint32_t ncells
 // bucket's range of the sorted LMS list, highest first.
 constexpr uint32_t LMS_DIGIT = 255;
 
-// Items carry the target position (low 32 bits) and the character in front
-// of it (bits 32..39), stored beside the entry in c0s, so that every entry's
-// predecessor character is gathered from the text once, in the same sector
-// read that finds the entry's own predecessor.
+// Items carry the target position (low 32 bits) and its predecessor window
+// (high 32 bits, win_next), stored beside the entry in wins: the decision
+// and the target bucket come from the window, and the text is read only
+// when an induced suffix's window has no look-ahead byte left.
 template <bool LSCAN> struct BucketPolicy {
     using Item = uint64_t;
     static constexpr int kMinBlocks = 3;
@@ -442,24 +447,24 @@ template <bool LSCAN> struct BucketPolicy {
     uint32_t *lms_out;   // S scan, LMS-substring round: sorted LMS list (else null)
     uint32_t lms_hi;     // index of this bucket's last entry in that list
     uint32_t lms_cap;    // entries of the list
-    uint8_t *c0s;        // c0s[slot] = text[sa[slot] - 1] for every placed entry
+    uint32_t *wins;      // wins[slot] = predecessor window of sa[slot] for every placed entry
     struct Pre {
         uint32_t x;
-        uint32_t c0;
+        uint32_t w;
     };
     __device__ __forceinline__ void pre(uint64_t i, Pre &p) const {
         const uint32_t slot = seq.slot((uint32_t)i);
         p.x = sa[slot];
-        p.c0 = c0s[slot];
+        p.w = wins[slot];
     }
     __device__ __forceinline__ void load(uint64_t i, const Pre &p, Item &it, uint32_t &d) const {
         const uint32_t x = p.x;
         d = 256;
         if (x > 0) {
-            uint32_t c0 = p.c0;
+            const uint32_t c0 = p.w & 0xFFu;
             if (LSCAN ? c0 > c : c0 < c) {
                 d = c0;
-                it = (uint64_t)(x - 1) | ((uint64_t)(x >= 2 ? text[x - 2] : 0) << 32);
+                it = (uint64_t)(x - 1) | (uint64_t)win_next(p.w, text, x) << 32;
             } else if (!LSCAN && lms_out && c0 > c && i < seq.a_len) {
                 d = LMS_DIGIT;
                 it = x;
@@ -478,7 +483,7 @@ template <bool LSCAN> struct BucketPolicy {
         }
         if (idx < n) {
             sa[idx] = (uint32_t)it;
-            c0s[idx] = (uint8_t)(it >> 32);
+            wins[idx] = (uint32_t)(it >> 32);
         } else {
             dev_fail(err, DEVERR_RANGE);
         }
@@ -504,7 +509,7 @@ static inline uint32_t grid_cap(uint64_t n, uint32_t cap) {
 // the part; fills the remaining part - nseeds slots.
 static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint32_t start, int dir, uint32_t nseeds,
                               uint32_t part, uint8_t c, uint32_t *subx, uint32_t *subr, uint8_t *sube, uint32_t *off,
-                              uint8_t *c0s, cudaStream_t s) {
+                              uint32_t *wins, cudaStream_t s) {
     if (part == 0) return PSACAK_OK;
     if (nseeds == 0 || nseeds > part)
         return set_error(PSACAK_EINTERNAL, "bucket %u: %u seeds for a part of %u", c, nseeds, part);
@@ -513,8 +518,8 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     const uint32_t cells = part - nseeds;
     // step 1: depth-1 cells and the sub-list of runs >= 2
     ChainPair *d_pair = (ChainPair *)(ctx.d_scalars + 24);
-    PSK_TRY((ctx.scan<ChainPair, OpPair>(SeedLoad{text, sa, c0s, start, dir, c},
-                                         SeedStore{sa, c0s, subx, subr, sube, first, cells, dir, c, ctx.d_err}, nseeds,
+    PSK_TRY((ctx.scan<ChainPair, OpPair>(SeedLoad{text, sa, wins, start, dir, c},
+                                         SeedStore{sa, wins, subx, subr, sube, first, cells, dir, c, ctx.d_err}, nseeds,
                                          d_pair, OpPair(), "chain_seeds")));
     uint32_t h[5];
     PSK_TRY(ctx.read_u32((const uint32_t *)d_pair, h, 2));
@@ -536,7 +541,7 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     const uint32_t sfirst = dir > 0 ? first + C1 : first - C1;
     const uint32_t direct = D1 + D2 + D3;
     PSK_TRY((ctx.scan<ChainCounts, OpChain>(ChainLoad{subx, subr, sube},
-                                            ChainStore{sa, c0s, ndeep ? off : nullptr, sfirst, D1, D1 + D2, direct, dir,
+                                            ChainStore{sa, wins, ndeep ? off : nullptr, sfirst, D1, D1 + D2, direct, dir,
                                                        c, ctx.d_err},
                                             m, (ChainCounts *)nullptr, OpChain(), "chain_place")));
     if (ndeep == 0) return PSACAK_OK;
@@ -558,7 +563,7 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
     const uint32_t dfirst = dir > 0 ? sfirst + direct : sfirst - direct;
     PSK_PROF_LAUNCH(s, "chain_place_deep", ndeep, 13ull * ndeep,
                     (k_place_cells<<<grid_cap(ndeep, 8192), 256, 0, s>>>(in1 ? v1.get() : v0.get(), ndeep, dfirst, dir,
-                                                                          sa, c0s)));
+                                                                          sa, wins)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -567,7 +572,7 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
 // cur[256..512) (the caller swaps the halves afterwards).
 template <bool LSCAN>
 static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t n, BucketSeq seq, uint8_t c,
-                           const uint32_t *cur_in, uint32_t *cur_out, uint8_t *c0s, cudaStream_t s,
+                           const uint32_t *cur_in, uint32_t *cur_out, uint32_t *wins, cudaStream_t s,
                            uint32_t *lms_out = nullptr, uint32_t lms_hi = 0, uint32_t lms_cap = 0) {
     uint32_t nitems = seq.a_len + seq.b_len;
     if (nitems == 0) {
@@ -576,16 +581,16 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
     }
     PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 8 * OS_BLOCK) + 1));
     BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err, lms_out, lms_hi, lms_cap,
-                            c0s};
-    // algorithmic bytes: each entry and its c0 read (5); inducing entries
-    // write entry + c0 (5, added from the device count) and read the text
-    // byte in front of their target (1, with it).
+                            wins};
+    // algorithmic bytes: each entry and its window read (8); inducing
+    // entries write entry + window (8, added from the device count) and read
+    // the text byte in front of their target (1, with it).
     return onesweep_ipt<BucketPolicy<LSCAN>>(pol, nitems, ctx.tile_ipt(), ctx.os, ctx.d_err, s, "induce_scatter",
-                                              5ull * nitems);
+                                              8ull * nitems);
 }
 
 status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_t *lms, const ByteGeom &hg,
-                        const ByteGeom *dgeom, InduceMode mode, const uint64_t *sorted_pc, uint64_t n1,
+                        const ByteGeom *dgeom, InduceMode mode, const uint64_t *sorted_win, uint64_t n1,
                         uint32_t *sa, cudaStream_t s, uint32_t *lms_out) {
     uint32_t maxpart = 1, maxbucket = 1;
     for (int c = 0; c < 256; c++) {
@@ -595,11 +600,12 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         maxpart = hg.scount[c] > maxpart ? hg.scount[c] : maxpart;
     }
     DBuf<uint32_t> cur, cur2, runs, off, subx;
-    DBuf<uint8_t> endc, c0s;
+    DBuf<uint8_t> endc;
+    DBuf<uint32_t> wins;
     PSK_TRY(cur.init(ctx, 512));
     PSK_TRY(cur2.init(ctx, 512));
     PSK_TRY(endc.init(ctx, maxpart));
-    PSK_TRY(c0s.init(ctx, n));
+    PSK_TRY(wins.init(ctx, n));
     PSK_TRY(runs.init(ctx, maxpart));
     PSK_TRY(subx.init(ctx, maxpart));
     PSK_TRY(off.init(ctx, maxpart));
@@ -613,14 +619,14 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         const uint64_t G = ceil_div(nwords, 2048) < 4ull * ctx.scan_ctas ? ceil_div(nwords, 2048) : 4ull * ctx.scan_ctas;
         const uint64_t wchunk = ceil_div(nwords, G);
         PSK_PROF_LAUNCH(s, "place_lms", nwords, 0,
-                        (k_place_lms_any8<<<(uint32_t)G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, c0s.get(),
+                        (k_place_lms_any8<<<(uint32_t)G, PL_BLOCK, 0, s>>>(text, nwords, lms, dgeom, curL, sa, wins.get(),
                                                                          wchunk)));
     } else if (n1 > 0) {
         PSK_PROF_LAUNCH(s, "place_lms", n1, 0,
-                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(sorted_pc, n1, dgeom, sa,
-                                                                                  c0s.get())));
+                        (k_place_lms_sorted8<<<grid_cap(n1, 8192), 256, 0, s>>>(sorted_win, n1, dgeom, sa,
+                                                                                  wins.get())));
     }
-    k_init_cursors<<<1, 256, 0, s>>>(dgeom, text, n, curL, curS, sa, c0s.get());
+    k_init_cursors<<<1, 256, 0, s>>>(dgeom, text, n, curL, curS, sa, wins.get());
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
 
@@ -632,10 +638,10 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (lc > 0) {
             uint32_t cl = 0;
             PSK_TRY(ctx.read_u32(curL + c, &cl));
-            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, subx, runs, endc, off, c0s, s));
+            PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, subx, runs, endc, off, wins, s));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
-        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, c0s, s));
+        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, wins, s));
         std::swap(curL, alt);
     }
     alt = cur2.get() + 256;
@@ -647,12 +653,12 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         if (sc > 0) {
             uint32_t cs = 0;
             PSK_TRY(ctx.read_u32(curS + c, &cs));
-            PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, subx, runs, endc, off, c0s,
+            PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, subx, runs, endc, off, wins,
                                   s));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
         const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;
-        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, c0s, s, extract ? lms_out : nullptr,
+        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, wins, s, extract ? lms_out : nullptr,
                                   hg.lmsstart[c] + hg.lmscount[c] - 1, (uint32_t)n1));
         std::swap(curS, alt);
     }

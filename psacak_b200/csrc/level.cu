@@ -451,7 +451,7 @@ status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint
 }
 
 // Byte levels: the permuted list carries each LMS position's predecessor
-// character, (p << 8) | text[p - 1], so that the final placement needs no
+// window, p | win_fill(text, p) << 32, so that the final placement needs no
 // gather from the text.
 __global__ void k_lms_list8(const uint8_t *__restrict__ text, const uint32_t *__restrict__ lms,
                             const uint32_t *__restrict__ pref, uint64_t nwords, uint64_t *plist) {
@@ -461,7 +461,7 @@ __global__ void k_lms_list8(const uint8_t *__restrict__ text, const uint32_t *__
         while (word) {
             int b = __ffs(word) - 1;
             const uint64_t p = (w << 5) + b;  // LMS positions are > 0
-            plist[o++] = (p << 8) | text[p - 1];
+            plist[o++] = p | (uint64_t)win_fill(text, (uint32_t)p) << 32;
             word &= word - 1;
         }
     }
@@ -477,7 +477,7 @@ __global__ void k_permute8(const uint32_t *__restrict__ sa1, uint64_t n1, const 
 #pragma unroll
         for (int u = 0; u < U; u++) r[u] = i0 + u * stride < n1 ? sa1[i0 + u * stride] : 0u;
 #pragma unroll
-        for (int u = 0; u < U; u++) v[u] = r[u] < n1 ? plist[r[u]] : (1ull << 8);
+        for (int u = 0; u < U; u++) v[u] = r[u] < n1 ? plist[r[u]] : 1ull;
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const uint64_t i = i0 + u * stride;

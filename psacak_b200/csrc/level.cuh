@@ -70,9 +70,38 @@ status_t translate_names(uint32_t *red, uint64_t n1, const uint32_t *types, cons
 status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint32_t *lms_pref, uint64_t n,
                      uint32_t *plist, uint32_t *err, cudaStream_t s);
 
-// Byte levels: out[i] = (P[sa1[i]] << 8) | text[P[sa1[i]] - 1], the permuted
-// LMS positions with their predecessor characters.  `plist` is scratch of
-// n1 entries.
+// Predecessor window of a byte-level SA entry x > 0, kept beside the entry
+// by the bucket scans: byte 0 = text[x-1] (the character that decides
+// whether x induces x-1 and into which bucket), bytes 1 and 2 = text[x-2]
+// and text[x-3], bits 24..25 = how many of those two look-ahead bytes are
+// valid.  The window of x-1 is this one shifted by a byte while a
+// look-ahead byte is left, so only every third step of an induction chain
+// reads the text (three adjacent bytes, one sector).  Bytes of positions
+// below 0 are 0 and never used: entry 0 induces nothing.
+constexpr uint32_t WIN_FULL = 2u << 24;
+__device__ __forceinline__ uint32_t win_fill(const uint8_t *text, uint32_t x) {
+    const uint32_t a = text[x - 1];
+    const uint32_t b = x >= 2 ? text[x - 2] : 0u;
+    const uint32_t c = x >= 3 ? text[x - 3] : 0u;
+    return a | b << 8 | c << 16 | WIN_FULL;
+}
+// Window of x - 1 from the window w of x (x >= 1).
+__device__ __forceinline__ uint32_t win_next(uint32_t w, const uint8_t *text, uint32_t x) {
+    const uint32_t k = w >> 24;
+    if (k) return ((w >> 8) & 0xFFFFu) | ((k - 1) << 24);
+    return x >= 2 ? win_fill(text, x - 1) : 0u;
+}
+// Window of the suffix d characters into a run (1 <= d <= r) in front of a
+// suffix x: text[x-1 .. x-r] are c and text[x-r-1] is e.
+__device__ __forceinline__ uint32_t run_win(uint32_t d, uint32_t r, uint32_t c, uint32_t e) {
+    const uint32_t left = r - d;
+    const uint32_t b0 = left > 0 ? c : e, b1 = left > 1 ? c : e, b2 = left > 2 ? c : e;
+    return b0 | b1 << 8 | b2 << 16 | (left < 2 ? left : 2u) << 24;
+}
+
+// Byte levels: out[i] = P[sa1[i]] | win_fill(text, P[sa1[i]]) << 32, the
+// permuted LMS positions with their predecessor windows.  `plist` is
+// scratch of n1 entries.
 status_t permute_lms8(const uint32_t *sa1, uint64_t n1, const uint8_t *text, const uint32_t *lms,
                       const uint32_t *lms_pref, uint64_t n, uint64_t *plist, uint64_t *out, uint32_t *err,
                       cudaStream_t s);
