@@ -450,6 +450,10 @@ def run_b200(args):
             e2e_s = float(t.item())
         e2e = {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n, "d2h_bytes_per_step": 4 * n,
                "ms_per_step": 1000.0 * e2e_s, "api": "psacak8_ctx (host pointers, pinned buffers)"}
+        if not args.no_verify:
+            # the host copy (sent bucket part by bucket part during the final
+            # scans) must equal the checked device-resident array
+            e2e["verified"] = bool(verified) and bool(np.array_equal(hs, d_sa.cpu().numpy().view(np.uint32)))
 
     cpu = cpu_all = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -534,8 +534,10 @@ status_t ctx_init(Ctx &c, int device) {
     PSK_CUDA(cudaMemPoolCreate(&c.pool, &props));
     uint64_t thresh = UINT64_MAX;
     PSK_CUDA(cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh));
-    PSK_CUDA(cudaMallocHost(&c.h_pinned, 4096));
-    PSK_CUDA(cudaMallocHost(&c.h_hist, RADIX_MAX_PASSES * 256 * sizeof(uint32_t)));
+    PSK_CUDA(cudaHostAlloc(&c.h_pinned, 4096, cudaHostAllocMapped));
+    PSK_CUDA(cudaHostAlloc(&c.h_hist, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), cudaHostAllocMapped));
+    PSK_CUDA(cudaHostGetDevicePointer(&c.m_pinned, c.h_pinned, 0));
+    PSK_CUDA(cudaHostGetDevicePointer(&c.m_hist, c.h_hist, 0));
     PSK_CUDA(cudaMalloc(&c.os.tickets, 64 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_hist, 256 * RADIX_MAX_CTAS * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
@@ -561,6 +563,8 @@ void ctx_free(Ctx &c) {
     c.ss.max_tiles = 0;
     c.os.tickets = nullptr;
     c.h_hist = nullptr;
+    c.m_hist = nullptr;
+    c.m_pinned = nullptr;
     if (c.d_hist) cudaFree(c.d_hist);
     if (c.d_scalars) cudaFree(c.d_scalars);
     if (c.d_err) cudaFree(c.d_err);
@@ -571,6 +575,13 @@ void ctx_free(Ctx &c) {
     if (c.pool) cudaMemPoolDestroy(c.pool);
     c.pool = nullptr;
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
+    if (c.copy_stream) {
+        cudaStreamSynchronize(c.copy_stream);
+        cudaStreamDestroy(c.copy_stream);
+    }
+    if (c.copy_ev) cudaEventDestroy(c.copy_ev);
+    c.copy_stream = nullptr;
+    c.copy_ev = nullptr;
     c.h_pinned = nullptr;
 }
 
@@ -649,8 +660,27 @@ status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_
     PSK_TRY(dt.init(c, n));
     PSK_TRY(ds.init(c, n));
     if (n) PSK_CUDA(cudaMemcpyAsync(dt.get(), text, n * sizeof(C), cudaMemcpyHostToDevice, c.stream));
-    PSK_TRY(run_dev<C>(c, dt.get(), n, ds.get(), c.own_stream, sched));
-    if (n) PSK_CUDA(cudaMemcpyAsync(sa, ds.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+    // A pinned output buffer receives the byte-level SA bucket part by bucket
+    // part during the final scans (Ctx::sink_part); pageable memory would
+    // make each of those copies wait for itself on the host.
+    bool sink = false;
+    if constexpr (sizeof(C) == 1) {
+        cudaPointerAttributes pa{};
+        if (n && cudaPointerGetAttributes(&pa, sa) == cudaSuccess && pa.type == cudaMemoryTypeHost) {
+            if (!c.copy_stream) PSK_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+            if (!c.copy_ev) PSK_CUDA(cudaEventCreateWithFlags(&c.copy_ev, cudaEventDisableTiming));
+            c.sink_dev = ds.get();
+            c.sink_host = sa;
+            sink = true;
+        }
+        cudaGetLastError();  // a pointer query on pageable memory may leave an error behind
+    }
+    c.sink_done = false;
+    const status_t st = run_dev<C>(c, dt.get(), n, ds.get(), c.own_stream, sched);
+    c.sink_dev = c.sink_host = nullptr;
+    if (sink) PSK_CUDA(cudaStreamSynchronize(c.copy_stream));  // before ds goes back to the arena
+    PSK_TRY(st);
+    if (n && !c.sink_done) PSK_CUDA(cudaMemcpyAsync(sa, ds.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
     dt.reset();
     ds.reset();
     PSK_TRY(c.sync());

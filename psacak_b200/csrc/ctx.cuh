@@ -20,11 +20,13 @@ struct Ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;  // stream of the current call
     cudaMemPool_t pool = nullptr;
-    uint32_t *h_pinned = nullptr;   // small pinned buffer for scalar read-backs
+    uint32_t *h_pinned = nullptr;   // small pinned, mapped buffer for scalar read-backs
+    uint32_t *m_pinned = nullptr;   // its device view
     uint32_t *d_hist = nullptr;     // 256 * RADIX_MAX_CTAS radix histograms
     uint32_t *d_scalars = nullptr;  // 64 device scalars
     uint32_t *d_err = nullptr;      // device error word
-    uint32_t *h_hist = nullptr;     // pinned copy of the radix digit counts
+    uint32_t *h_hist = nullptr;     // pinned, mapped copy of the radix digit counts
+    uint32_t *m_hist = nullptr;     // its device view
     OnesweepScratch os;             // look-back status words of the onesweep kernels
     ScanScratch ss;                 // look-back flags and values of the single-pass scans
     uint32_t scan_ctas = 0;         // CTAs of the grid-stride helper kernels
@@ -41,6 +43,24 @@ struct Ctx {
     Profiler prof;
     unsigned long long *d_induced = nullptr;  // entries scattered by the bucket scans
     std::mutex mu;
+
+    // Host destination of the final suffix array, set by host-pointer calls
+    // whose output buffer is pinned: the level-0 bucket scans send each
+    // bucket part to it as soon as that part is final (on copy_stream, after
+    // an event on the build stream), so the copy overlaps the rest of the
+    // build.  sink_done tells the caller that every slot was sent.
+    uint32_t *sink_dev = nullptr, *sink_host = nullptr;
+    bool sink_done = false;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev = nullptr;
+    status_t sink_part(uint64_t first, uint64_t count) {
+        if (count == 0) return PSACAK_OK;
+        PSK_CUDA(cudaEventRecord(copy_ev, stream));
+        PSK_CUDA(cudaStreamWaitEvent(copy_stream, copy_ev, 0));
+        PSK_CUDA(cudaMemcpyAsync(sink_host + first, sink_dev + first, count * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, copy_stream));
+        return PSACAK_OK;
+    }
 
     // Workspace arena: one device buffer reused by every build.  Blocks are
     // carved from the top and released stack-wise (a block freed out of
@@ -119,9 +139,8 @@ struct Ctx {
     }
     // Copies `count` uint32 from device to host and waits for the stream.
     status_t read_u32(const uint32_t *d, uint32_t *h, size_t count = 1) {
-        PSK_CUDA(cudaMemcpyAsync(h_pinned, d, count * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        PSK_CUDA(cudaStreamSynchronize(stream));
-        for (size_t i = 0; i < count; i++) h[i] = h_pinned[i];
+        PSK_TRY(read_back(d, m_pinned, (uint32_t)count, stream));
+        for (size_t i = 0; i < count; i++) h[i] = ((volatile uint32_t *)h_pinned)[i];
         return PSACAK_OK;
     }
     // Debug aid: when stage timing is on, waits for the stream and prints the
@@ -184,7 +203,7 @@ struct Ctx {
     template <class K, class V>
     status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1, bool hist_ready = false) {
         PSK_TRY(ensure_onesweep(ceil_div(n, 8 * OS_BLOCK) + 1));
-        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, os, d_err, in1, stream, RADIX_IPT,
+        return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, m_hist, os, d_err, in1, stream, RADIX_IPT,
                                       hist_ready);
     }
     // Single-pass stable compaction (see compact1).

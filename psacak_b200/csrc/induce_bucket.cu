@@ -576,7 +576,9 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
                            uint32_t *lms_out = nullptr, uint32_t lms_hi = 0, uint32_t lms_cap = 0) {
     uint32_t nitems = seq.a_len + seq.b_len;
     if (nitems == 0) {
-        PSK_CUDA(cudaMemcpyAsync(cur_out, cur_in, 256 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        k_copy_words<<<1, 256, 0, s>>>(cur_in, cur_out, 256);
+        PSK_KCOUNT();
+        PSK_LAUNCH_CHECK();
         return PSACAK_OK;
     }
     PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 8 * OS_BLOCK) + 1));
@@ -630,6 +632,11 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
 
+    // The final SA goes to the host while the scans run: a bucket's L part
+    // is final once its chains are expanded in the L scan (later writes go
+    // to larger buckets or to S parts), its S part once its chains are
+    // expanded in the S scan.
+    const bool sink = mode == INDUCE_FINAL && ctx.sink_host && sa == ctx.sink_dev;
     // L scan: buckets in increasing order.
     for (int c = 0; c < 256; c++) {
         const uint32_t head = hg.head[c], tail = hg.tail[c];
@@ -639,6 +646,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
             uint32_t cl = 0;
             PSK_TRY(ctx.read_u32(curL + c, &cl));
             PSK_TRY(expand_chains(ctx, text, sa, head, +1, cl - head, lc, (uint8_t)c, subx, runs, endc, off, wins, s));
+            if (sink) PSK_TRY(ctx.sink_part(head, lc));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
         PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, wins, s));
@@ -655,6 +663,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
             PSK_TRY(ctx.read_u32(curS + c, &cs));
             PSK_TRY(expand_chains(ctx, text, sa, tail - 1, -1, tail - cs, sc, (uint8_t)c, subx, runs, endc, off, wins,
                                   s));
+            if (sink) PSK_TRY(ctx.sink_part(head + lc, sc));
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
         const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;
@@ -662,6 +671,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
                                   hg.lmsstart[c] + hg.lmscount[c] - 1, (uint32_t)n1));
         std::swap(curS, alt);
     }
+    if (sink) ctx.sink_done = true;
     return PSACAK_OK;
 }
 

@@ -31,6 +31,19 @@ status_t cuda_status(cudaError_t e, const char *what, const char *file, int line
 const char *last_error() { return t_last_error; }
 void clear_error() { t_last_error[0] = 0; }
 
+__global__ void k_copy_words(const uint32_t *__restrict__ src, uint32_t *dst, uint32_t count) {
+    for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) dst[i] = src[i];
+}
+
+status_t read_back(const uint32_t *d, uint32_t *mapped, uint32_t count, cudaStream_t s) {
+    if (count == 0) return PSACAK_OK;
+    k_copy_words<<<1, 256, 0, s>>>(d, mapped, count);
+    PSK_KCOUNT();
+    PSK_CUDA(cudaGetLastError());
+    PSK_CUDA(cudaStreamSynchronize(s));
+    return PSACAK_OK;
+}
+
 __global__ void k_radix_bases(const uint32_t *hist, uint32_t *bases) {
     __shared__ uint32_t smem[33];
     const uint32_t p = blockIdx.x;

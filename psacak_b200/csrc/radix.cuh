@@ -247,12 +247,22 @@ __device__ __forceinline__ void radix_flush_digits(const uint32_t *sh, int npass
 // Exclusive digit bases per pass (one block of 256 threads per pass).
 __global__ void k_radix_bases(const uint32_t *hist, uint32_t *bases);
 
+// dst[i] = src[i] for i < count, by one block (small copies that must not
+// wait for a copy engine).
+__global__ void k_copy_words(const uint32_t *__restrict__ src, uint32_t *dst, uint32_t count);
+
+// Reads `count` words back to the host: a one-block kernel stores them into
+// `mapped` (the device view of pinned, mapped host memory) and the stream is
+// synchronised.  Unlike a device-to-host memcpy this does not queue behind
+// bulk copies that a copy engine is working through on another stream.
+status_t read_back(const uint32_t *d, uint32_t *mapped, uint32_t count, cudaStream_t s);
+
 // When `hist_ready` is set, the producer of the keys has already counted
 // the digits of every pass into d_hist (see radix_count_digits), and the
 // histogram kernel is skipped.
 template <class K, class V>
 status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit, int end_bit, uint32_t *d_hist,
-                          uint32_t *h_hist, OnesweepScratch &sc, uint32_t *err, int *result_in_1, cudaStream_t s,
+                          uint32_t *h_hist, uint32_t *h_hist_mapped, OnesweepScratch &sc, uint32_t *err, int *result_in_1, cudaStream_t s,
                           int ipt = 12, bool hist_ready = false) {
     *result_in_1 = 0;
     if (n <= 1 || end_bit <= begin_bit) return PSACAK_OK;
@@ -267,8 +277,7 @@ status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit,
                             k0, n, begin_bit, npasses, end_bit, d_hist)));
     }
     PSK_PROF_LAUNCH(s, "radix_bases", npasses * 256, 0, (k_radix_bases<<<npasses, 256, 0, s>>>(d_hist, bases)));
-    PSK_CUDA(cudaMemcpyAsync(h_hist, d_hist, npasses * 256 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    PSK_CUDA(cudaStreamSynchronize(s));
+    PSK_TRY(read_back(d_hist, h_hist_mapped, npasses * 256, s));
     K *ki = k0, *ko = k1;
     V *vi = v0, *vo = v1;
     int flip = 0;
