@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "ctx.cuh"
+#include "hostio.cuh"
 #include "induce.cuh"
 #include "../../include/psacak_b200_debug.h"
 
@@ -582,6 +583,7 @@ void ctx_free(Ctx &c) {
     if (c.copy_ev) cudaEventDestroy(c.copy_ev);
     c.copy_stream = nullptr;
     c.copy_ev = nullptr;
+    host_stage_free(c);
     c.h_pinned = nullptr;
 }
 
@@ -659,28 +661,37 @@ status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_
     DBuf<uint32_t> ds;
     PSK_TRY(dt.init(c, n));
     PSK_TRY(ds.init(c, n));
-    if (n) PSK_CUDA(cudaMemcpyAsync(dt.get(), text, n * sizeof(C), cudaMemcpyHostToDevice, c.stream));
+    if (n) {
+        if (host_is_pinned(text))
+            PSK_CUDA(cudaMemcpyAsync(dt.get(), text, n * sizeof(C), cudaMemcpyHostToDevice, c.stream));
+        else
+            PSK_TRY(staged_upload(c, (char *)dt.get(), {HostPiece{(char *)text, 0, n * sizeof(C)}}, c.stream));
+    }
     // A pinned output buffer receives the byte-level SA bucket part by bucket
     // part during the final scans (Ctx::sink_part); pageable memory would
-    // make each of those copies wait for itself on the host.
+    // make each of those copies wait for itself on the host, so it is filled
+    // through the staging ring after the build.
+    const bool out_pinned = n && host_is_pinned(sa);
     bool sink = false;
-    if constexpr (sizeof(C) == 1) {
-        cudaPointerAttributes pa{};
-        if (n && cudaPointerGetAttributes(&pa, sa) == cudaSuccess && pa.type == cudaMemoryTypeHost) {
-            if (!c.copy_stream) PSK_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
-            if (!c.copy_ev) PSK_CUDA(cudaEventCreateWithFlags(&c.copy_ev, cudaEventDisableTiming));
-            c.sink_dev = ds.get();
-            c.sink_host = sa;
-            sink = true;
-        }
-        cudaGetLastError();  // a pointer query on pageable memory may leave an error behind
+    if (sizeof(C) == 1 && out_pinned) {
+        if (!c.copy_stream) PSK_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+        if (!c.copy_ev) PSK_CUDA(cudaEventCreateWithFlags(&c.copy_ev, cudaEventDisableTiming));
+        c.sink_dev = ds.get();
+        c.sink_host = sa;
+        sink = true;
     }
     c.sink_done = false;
     const status_t st = run_dev<C>(c, dt.get(), n, ds.get(), c.own_stream, sched);
     c.sink_dev = c.sink_host = nullptr;
     if (sink) PSK_CUDA(cudaStreamSynchronize(c.copy_stream));  // before ds goes back to the arena
     PSK_TRY(st);
-    if (n && !c.sink_done) PSK_CUDA(cudaMemcpyAsync(sa, ds.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+    if (n && !c.sink_done) {
+        if (out_pinned)
+            PSK_CUDA(cudaMemcpyAsync(sa, ds.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+        else
+            PSK_TRY(staged_download(c, (const char *)ds.get(), {HostPiece{(char *)sa, 0, n * sizeof(uint32_t)}},
+                                    c.stream));
+    }
     dt.reset();
     ds.reset();
     PSK_TRY(c.sync());
@@ -933,15 +944,42 @@ int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const uint64_t *
              ? PSACAK_OK
              : PSACAK_ENOMEM;
     if (st == PSACAK_OK) {
-        for (uint32_t i = 0; i < n_texts && st == PSACAK_OK; i++)
-            if (lens[i] && cudaMemcpyAsync(dt + off[i], texts[i], lens[i], cudaMemcpyHostToDevice, c.own_stream) !=
-                               cudaSuccess)
-                st = set_error(PSACAK_ECUDA, "batch upload of text %u failed", i);
+        // pinned buffers are copied directly; any pageable one sends the
+        // whole batch through the staging ring (hostio.cuh)
+        std::vector<HostPiece> tp, sp;
+        bool t_pinned = true, s_pinned = true;
+        for (uint32_t i = 0; i < n_texts; i++) {
+            if (!lens[i]) continue;
+            tp.push_back(HostPiece{(char *)texts[i], off[i], lens[i]});
+            sp.push_back(HostPiece{(char *)sas[i], off[i] * sizeof(uint32_t), lens[i] * sizeof(uint32_t)});
+            t_pinned = t_pinned && host_is_pinned(texts[i]);
+            s_pinned = s_pinned && host_is_pinned(sas[i]);
+        }
+        {
+            std::lock_guard<std::mutex> g(c.mu);
+            if (!t_pinned) {
+                st = staged_upload(c, (char *)dt, tp, c.own_stream);
+            } else {
+                for (const HostPiece &p : tp)
+                    if (st == PSACAK_OK &&
+                        cudaMemcpyAsync(dt + p.dev_off, p.host, p.bytes, cudaMemcpyHostToDevice, c.own_stream) !=
+                            cudaSuccess)
+                        st = set_error(PSACAK_ECUDA, "batch upload failed");
+            }
+        }
         if (st == PSACAK_OK) st = psacak8_batch_dev(ctx, dt, off.data(), n_texts, ds, c.own_stream, sched);
-        for (uint32_t i = 0; i < n_texts && st == PSACAK_OK; i++)
-            if (lens[i] && cudaMemcpyAsync(sas[i], ds + off[i], lens[i] * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                           c.own_stream) != cudaSuccess)
-                st = set_error(PSACAK_ECUDA, "batch download of SA %u failed", i);
+        if (st == PSACAK_OK) {
+            std::lock_guard<std::mutex> g(c.mu);
+            if (!s_pinned) {
+                st = staged_download(c, (const char *)ds, sp, c.own_stream);
+            } else {
+                for (const HostPiece &p : sp)
+                    if (st == PSACAK_OK &&
+                        cudaMemcpyAsync(p.host, (const char *)ds + p.dev_off, p.bytes, cudaMemcpyDeviceToHost,
+                                        c.own_stream) != cudaSuccess)
+                        st = set_error(PSACAK_ECUDA, "batch download failed");
+            }
+        }
     } else {
         set_error(PSACAK_ENOMEM, "batch: device allocation failed");
     }

@@ -15,6 +15,8 @@ struct psacak_ctx;
 
 namespace psk {
 
+struct HostStage;  // staging ring and host copy threads (hostio.cu)
+
 struct Ctx {
     Device dev;
     cudaStream_t own_stream = nullptr;
@@ -53,6 +55,7 @@ struct Ctx {
     bool sink_done = false;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev = nullptr;
+    HostStage *stage = nullptr;  // pageable host transfers (hostio.cuh), created on first use
     status_t sink_part(uint64_t first, uint64_t count) {
         if (count == 0) return PSACAK_OK;
         PSK_CUDA(cudaEventRecord(copy_ev, stream));

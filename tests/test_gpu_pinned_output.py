@@ -54,3 +54,42 @@ def test_pinned_and_pageable_agree_back_to_back():
     pk.psacak_inplace(t, c)
     assert (a == b).all() and (b == c).all()
     assert (b == o.psacak8(t)).all()
+
+
+def test_pageable_buffers_go_through_the_staging_ring():
+    """Pageable text and SA buffers larger than the two 64 MiB staging slots
+    (several chunks each way, a chunk boundary inside the buffers) give the
+    same array as pinned buffers, and the array passes the device check."""
+    t = synth.genome(150_000_000, seed=11)
+    page = np.empty(t.size, np.uint32)
+    pk.psacak_inplace(np.array(t), page)
+    pin = pinned_u32(t.size)
+    pk.psacak_inplace(t, pin)
+    assert (page == pin).all()
+    with pk.Context(0) as ctx:
+        dt = torch.from_numpy(t).cuda()
+        ds = torch.from_numpy(page.view(np.int32)).cuda()
+        assert ctx.check_sa8_dev(dt.data_ptr(), t.size, ds.data_ptr())
+
+
+def test_batch_with_pageable_and_pinned_buffers():
+    rng = np.random.default_rng(12)
+    lens = rng.integers(0, 1_500_000, 200)
+    lens[::17] = 0
+    texts = [synth.genome(int(k), seed=100 + i) if k else np.zeros(0, np.uint8) for i, k in enumerate(lens)]
+    with pk.Context(0) as ctx:
+        got = ctx.psacak_batch(texts)  # pageable numpy buffers: staged
+        import ctypes
+        n = len(texts)
+        pins = [torch.empty(max(int(k), 1), dtype=torch.uint8, pin_memory=True).numpy()[:int(k)] for k in lens]
+        for p, tx in zip(pins, texts):
+            p[:] = tx
+        outs = [pinned_u32(int(k)) for k in lens]
+        tp = (ctypes.c_void_p * n)(*[p.ctypes.data for p in pins])
+        sp = (ctypes.c_void_p * n)(*[o_.ctypes.data for o_ in outs])
+        ln = (ctypes.c_uint64 * n)(*[int(k) for k in lens])
+        pk._raise(pk.lib().psacak8_batch(ctx.handle, tp, ln, n, sp, None))
+    for i in range(n):
+        assert (got[i] == outs[i]).all(), i
+    for i in (1, 5, 50, 199):
+        assert (got[i] == o.psacak8(texts[i])).all(), i
