@@ -19,6 +19,7 @@
 
 #include "ctx.cuh"
 #include "induce.cuh"
+#include "small.cuh"
 
 namespace psk {
 
@@ -54,20 +55,32 @@ __device__ __forceinline__ uint32_t text_of(const uint64_t *__restrict__ off, ui
 }
 
 // cat[q] for q in [0, N): text byte (shifted below v) or the separator 0.
-// Text i occupies [off[i] + i, off[i+1] + i) of the concatenation, its
-// separator the slot right after.
-__global__ void k_batch_pack(const uint8_t *__restrict__ src, const uint64_t *__restrict__ coff, uint32_t k,
-                             uint64_t N, uint32_t v, uint8_t *cat) {
+// The i-th text of the chunk occupies [coff[i], coff[i+1] - 1) of the
+// concatenation, its separator the slot right after; its bytes start at
+// src[soff[i]].
+__global__ void k_batch_pack(const uint8_t *__restrict__ src, const uint64_t *__restrict__ coff,
+                             const uint64_t *__restrict__ soff, uint32_t k, uint64_t N, uint32_t v, uint8_t *cat) {
     for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t i = text_of(coff, k, q);  // coff[i] = off[i] + i
+        uint32_t i = text_of(coff, k, q);
         uint64_t p = q - coff[i];
         uint64_t len = coff[i + 1] - coff[i] - 1;
         uint8_t c = 0;
         if (p < len) {
-            c = src[coff[i] - i + p];
+            c = src[soff[i] + p];
             if (c < v) c = (uint8_t)(c + 1);
         }
         cat[q] = c;
+    }
+}
+
+// The chunk's suffix arrays, back to back in `sorted` (the i-th text's at
+// [coff[i] - i, coff[i+1] - i - 1)), to each text's own offset soff[i].
+__global__ void k_batch_unpack(const uint32_t *__restrict__ sorted, const uint64_t *__restrict__ xoff,
+                               const uint64_t *__restrict__ soff, uint32_t k, uint64_t total, uint32_t *sas) {
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = text_of(xoff, k, q);
+        sas[soff[i] + (q - xoff[i])] = sorted[q];
     }
 }
 
@@ -94,26 +107,35 @@ struct SepEmit {
     }
 };
 
-// One chunk: texts [t0, t1) of the packed device input, SAs to the same
-// packed offsets of d_sas.
-static status_t batch_chunk(Ctx &ctx, const uint8_t *d_src, const uint64_t *h_off, uint32_t t0, uint32_t t1,
+// One chunk: the texts ids[0 .. k) of the packed device input (text t at
+// [h_off[t], h_off[t+1])), SAs to the same packed offsets of d_sas.
+static status_t batch_chunk(Ctx &ctx, const uint8_t *d_src, const uint64_t *h_off, const uint32_t *ids, uint32_t k,
                             uint32_t *d_sas, uint32_t v) {
     cudaStream_t s = ctx.stream;
-    const uint32_t k = t1 - t0;
-    const uint64_t base = h_off[t0];
-    const uint64_t total = h_off[t1] - base;
-    const uint64_t N = total + k;
-    std::vector<uint64_t> coff(k + 1);
-    for (uint32_t i = 0; i <= k; i++) coff[i] = h_off[t0 + i] - base + i;
-    DBuf<uint64_t> dcoff;
+    // host tables: coff (with separators), xoff (without), soff (source offsets)
+    std::vector<uint64_t> tab(3 * (size_t)k + 2);
+    uint64_t *coff = tab.data(), *xoff = coff + k + 1, *soff = xoff + k + 1;
+    bool contiguous = true;
+    coff[0] = xoff[0] = 0;
+    for (uint32_t i = 0; i < k; i++) {
+        const uint64_t len = h_off[ids[i] + 1] - h_off[ids[i]];
+        coff[i + 1] = coff[i] + len + 1;
+        xoff[i + 1] = xoff[i] + len;
+        soff[i] = h_off[ids[i]];
+        if (i > 0 && ids[i] != ids[i - 1] + 1) contiguous = false;
+    }
+    const uint64_t total = xoff[k];
+    const uint64_t N = coff[k];
+    DBuf<uint64_t> dtab;
     DBuf<uint8_t> cat;
-    DBuf<uint32_t> sa, k0, v0, k1;
-    PSK_TRY(dcoff.init(ctx, k + 1));
-    PSK_CUDA(cudaMemcpyAsync(dcoff.get(), coff.data(), (k + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    DBuf<uint32_t> sa, k0, v0, k1, v1;
+    PSK_TRY(dtab.init(ctx, tab.size()));
+    PSK_CUDA(cudaMemcpyAsync(dtab.get(), tab.data(), tab.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    const uint64_t *dcoff = dtab.get(), *dxoff = dcoff + k + 1, *dsoff = dxoff + k + 1;
     PSK_TRY(cat.init(ctx, N));
     uint64_t g = ceil_div(N, 256);
     PSK_PROF_LAUNCH(s, "batch_pack", N, 2 * N,
-                    (k_batch_pack<<<(uint32_t)(g < 16384 ? g : 16384), 256, 0, s>>>(d_src + base, dcoff, k, N, v,
+                    (k_batch_pack<<<(uint32_t)(g < 16384 ? g : 16384), 256, 0, s>>>(d_src, dcoff, dsoff, k, N, v,
                                                                                    cat)));
     PSK_TRY(sa.init(ctx, N));
     PSK_TRY(build_level<uint8_t>(ctx, cat.get(), nullptr, nullptr, 256, N, sa, 0));
@@ -127,19 +149,58 @@ static status_t batch_chunk(Ctx &ctx, const uint8_t *d_src, const uint64_t *h_of
     if (got != total) return set_error(PSACAK_EINTERNAL, "batch: %u suffixes after dropping separators, expected %llu",
                                        got, (unsigned long long)total);
     // stable sort by text id: the values become every text's SA in order
+    // (written in place when the chunk's texts are adjacent in d_sas)
     int in1 = 0;
-    uint32_t *out = d_sas + base;
+    uint32_t *out = d_sas + soff[0];
+    if (!contiguous) {
+        PSK_TRY(v1.init(ctx, total));
+        out = v1.get();
+    }
     PSK_TRY((ctx.radix_sort<uint32_t, uint32_t>(k0, v0, k1, out, total, 0, bitlen(k > 1 ? k - 1 : 1), &in1)));
     if (!in1) PSK_CUDA(cudaMemcpyAsync(out, v0.get(), total * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    if (!contiguous) {
+        g = ceil_div(total, 256);
+        PSK_PROF_LAUNCH(s, "batch_unpack", total, 8 * total,
+                        (k_batch_unpack<<<(uint32_t)(g < 16384 ? g : 16384), 256, 0, s>>>(out, dxoff, dsoff, k, total,
+                                                                                        d_sas)));
+        PSK_LAUNCH_CHECK();
+    }
     return PSACAK_OK;
 }
 
 // Device form: texts packed back to back in d_texts (text i in
 // [h_off[i], h_off[i+1])), SAs written at the same offsets of d_sas.
+// Texts short enough for the direct prefix-doubling finisher (shorter than
+// the schedule's finish_below and at most SMALL_MAX bytes) are sorted one
+// CTA each in shared memory; the others by one build of their
+// concatenation (chunked).
 status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, uint32_t ntexts, uint32_t *d_sas) {
     cudaStream_t s = ctx.stream;
     const uint64_t total = h_off[ntexts] - h_off[0];
     if (total == 0) return PSACAK_OK;
+    std::vector<uint32_t> small, big;
+    for (uint32_t i = 0; i < ntexts; i++) {
+        const uint64_t len = h_off[i + 1] - h_off[i];
+        if (len == 0) continue;
+        if (len <= SMALL_MAX && ctx.sched.finish_below && len < ctx.sched.finish_below) small.push_back(i);
+        else big.push_back(i);
+    }
+    DBuf<uint64_t> d_off;
+    DBuf<uint32_t> d_ids;
+    if (!small.empty()) {
+        std::stable_sort(small.begin(), small.end(), [&](uint32_t a, uint32_t b) {
+            return h_off[a + 1] - h_off[a] > h_off[b + 1] - h_off[b];
+        });
+        PSK_TRY(d_off.init(ctx, (size_t)ntexts + 1));
+        PSK_TRY(d_ids.init(ctx, small.size()));
+        PSK_CUDA(cudaMemcpyAsync(d_off.get(), h_off, ((size_t)ntexts + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        PSK_CUDA(cudaMemcpyAsync(d_ids.get(), small.data(), small.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        PSK_TRY(small_sa<uint8_t>(ctx, d_texts, SmallJobs{d_off.get(), d_ids.get(), (uint32_t)small.size(), 0}, 256,
+                                  d_sas, s));
+        // the host tables must outlive the copies
+        PSK_CUDA(cudaStreamSynchronize(s));
+    }
+    if (big.empty()) return PSACAK_OK;
     // which byte values occur?
     uint32_t *mask = ctx.d_scalars + 16;
     PSK_CUDA(cudaMemsetAsync(mask, 0, 8 * sizeof(uint32_t), s));
@@ -159,26 +220,25 @@ status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, ui
     if (chunk > limit) chunk = limit;
     if (v == 256) {
         // all byte values in use: build every text on its own
-        for (uint32_t i = 0; i < ntexts; i++) {
+        for (uint32_t i : big) {
             uint64_t len = h_off[i + 1] - h_off[i];
-            if (len == 0) continue;
             PSK_TRY(build_level<uint8_t>(ctx, d_texts + h_off[i], nullptr, nullptr, 256, len, d_sas + h_off[i], 0));
         }
         return PSACAK_OK;
     }
-    uint32_t t0 = 0;
-    while (t0 < ntexts) {
-        uint32_t t1 = t0;
+    size_t t0 = 0;
+    while (t0 < big.size()) {
+        size_t t1 = t0;
         uint64_t acc = 0;
-        while (t1 < ntexts) {
-            uint64_t len = h_off[t1 + 1] - h_off[t1];
+        while (t1 < big.size()) {
+            uint64_t len = h_off[big[t1] + 1] - h_off[big[t1]];
             if (t1 > t0 && acc + len + 1 > chunk) break;
             acc += len + 1;
             t1++;
         }
-        if (acc > limit) return set_error(PSACAK_EINVAL, "batch text %u is too long (%llu bytes)", t0,
-                                          (unsigned long long)(h_off[t0 + 1] - h_off[t0]));
-        PSK_TRY(batch_chunk(ctx, d_texts, h_off, t0, t1, d_sas, v));
+        if (acc > limit) return set_error(PSACAK_EINVAL, "batch text %u is too long (%llu bytes)", big[t0],
+                                          (unsigned long long)(h_off[big[t0] + 1] - h_off[big[t0]]));
+        PSK_TRY(batch_chunk(ctx, d_texts, h_off, big.data() + t0, (uint32_t)(t1 - t0), d_sas, v));
         t0 = t1;
     }
     return PSACAK_OK;
