@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
         s_wcnt[ww][d] = (uint16_t)count;
         count += c;
     }
-    const uint32_t excl = os_lookback(status, tile, d, count, epoch, err);
+    const uint32_t excl = os_lookback<1>(status, tile, d, count, epoch, err);
     uint32_t ex, tot;
     block_scan<uint32_t, OpSum<uint32_t>, OS_BLOCK>(count, OpSum<uint32_t>(), s_scan, &ex, &tot);
     s_tstart[d] = ex;
