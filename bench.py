@@ -432,7 +432,7 @@ def run_b200(args):
         lib = pk.lib()
         import ctypes
         times = []
-        for i in range(args.e2e_steps + 1):
+        for i in range(max(args.warmup, 1) + args.e2e_steps):  # the same warm-up as the device-resident steps
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
@@ -441,7 +441,7 @@ def run_b200(args):
             dt = time.perf_counter() - t0
             if rc != 0:
                 pk._raise(rc)
-            if i > 0:
+            if i >= max(args.warmup, 1):
                 times.append(dt)
         e2e_s = float(np.mean(times))
         if dist:
@@ -599,7 +599,7 @@ def run_batch(args):
         ptrs_s = (ctypes.c_void_p * len(my_texts))(*[x.ctypes.data for x in h_sas])
         lens_c = (ctypes.c_uint64 * len(my_texts))(*[t.size for t in my_texts])
         times = []
-        for i in range(args.e2e_steps + 1):
+        for i in range(max(args.warmup, 1) + args.e2e_steps):  # the same warm-up as the device-resident steps
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
@@ -607,7 +607,7 @@ def run_batch(args):
             dt = time.perf_counter() - t0
             if rc != 0:
                 pk._raise(rc)
-            if i > 0:
+            if i >= max(args.warmup, 1):
                 times.append(dt)
         e2e_s = _max_over_ranks(torch, dist, dev, float(np.mean(times)))
         e2e = {"value": total_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n, "d2h_bytes_per_step": 4 * n,
@@ -790,14 +790,14 @@ def run_zipf32(args):
         h_text.numpy()[:] = text.view(np.int32)
         h_sa = torch.empty(n, dtype=torch.int32, pin_memory=True)
         times = []
-        for i in range(args.e2e_steps + 1):
+        for i in range(max(args.warmup, 1) + args.e2e_steps):  # the same warm-up as the device-resident steps
             t0 = time.perf_counter()
             rc = pk.lib().psacak32_ctx(ctx.handle, ctypes.c_void_p(h_text.data_ptr()), n,
                                        ctypes.c_void_p(h_sa.data_ptr()), None)
             dt = time.perf_counter() - t0
             if rc != 0:
                 pk._raise(rc)
-            if i > 0:
+            if i >= max(args.warmup, 1):
                 times.append(dt)
         e2e_s = _max_over_ranks(torch, dist, dev, float(np.mean(times)))
         e2e = {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n,

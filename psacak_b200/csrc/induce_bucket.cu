@@ -47,6 +47,12 @@ struct BucketSeq {
         q -= a_len;
         return dir > 0 ? b_start + q : b_start - q;
     }
+    // the same with the direction known at compile time (DIR = dir)
+    template <int DIR> __device__ __forceinline__ uint32_t slot_dir(uint32_t q) const {
+        const uint32_t s0 = q < a_len ? a_start : b_start;
+        const uint32_t qq = q < a_len ? q : q - a_len;
+        return DIR > 0 ? s0 + qq : s0 - qq;
+    }
 };
 
 // ---- placement of the LMS positions --------------------------------------
@@ -453,7 +459,7 @@ template <bool LSCAN> struct BucketPolicy {
         uint32_t w;
     };
     __device__ __forceinline__ void pre(uint64_t i, Pre &p) const {
-        const uint32_t slot = seq.slot((uint32_t)i);
+        const uint32_t slot = seq.template slot_dir<LSCAN ? 1 : -1>((uint32_t)i);
         p.x = sa[slot];
         p.w = wins[slot];
     }
@@ -471,9 +477,12 @@ template <bool LSCAN> struct BucketPolicy {
             }
         }
     }
-    __device__ __forceinline__ uint64_t out(uint32_t d, uint64_t r) const {
-        if (!LSCAN && lms_out && d == LMS_DIGIT) return (uint64_t)lms_hi - r;
-        return LSCAN ? (uint64_t)cur_in[d] + r : (uint64_t)cur_in[d] - 1 - r;
+    // rank r of digit d goes to cur_in[d] + r (L), cur_in[d] - 1 - r (S) or,
+    // for the extracted LMS suffixes, lms_hi - r
+    static constexpr int kOutSign = LSCAN ? 1 : -1;
+    __device__ __forceinline__ uint64_t out0(uint32_t d) const {
+        if (!LSCAN && lms_out && d == LMS_DIGIT) return (uint64_t)lms_hi;
+        return LSCAN ? (uint64_t)cur_in[d] : (uint64_t)cur_in[d] - 1;
     }
     __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t d) const {
         if (!LSCAN && lms_out && d == LMS_DIGIT) {

@@ -19,9 +19,9 @@
 //
 // A Policy supplies, per item index i < n:
 //   load(i, item, digit)            -> digit in [0, 256) or >= 256 to drop it
-//   out(digit, rank)                -> output index of the rank-th item of
-//                                      that digit (rank counts from 0 over all
-//                                      tiles of this launch)
+//   out0(digit), kOutSign (+1 / -1) -> the rank-th item of a digit (rank
+//                                      counting from 0 over all tiles of this
+//                                      launch) goes to out0(digit) + kOutSign * rank
 //   store(index, item, digit)
 //   finish(digit, total)            -> called once per digit by the last tile
 //   kMinBlocks                      -> CTAs per SM the register budget must allow
@@ -121,9 +121,8 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
     extern __shared__ __align__(16) unsigned char os_smem[];
     Item *s_item = (Item *)os_smem;
     uint8_t *s_dig = (uint8_t *)(s_item + TILE);
-    __shared__ uint32_t s_excl[256];
     __shared__ uint32_t s_tstart[256];
-    __shared__ uint32_t s_tcount[256];
+    __shared__ uint64_t s_obase[256];  // output index of tile position i = s_obase[digit] + kOutSign * i
     __shared__ uint16_t s_wcnt[OS_WARPS][256];
     __shared__ uint32_t s_scan[33];
     __shared__ uint32_t s_tile;
@@ -137,6 +136,7 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint64_t base = (uint64_t)tile * TILE;
+    const uint32_t cnt = n - base < (uint64_t)TILE ? (uint32_t)(n - base) : (uint32_t)TILE;  // items of this tile
 
     // load every item of the thread first (independent loads in flight);
     // two-phase policies read their direct operands for every item before
@@ -147,21 +147,21 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
         typename Policy::Pre pre[IPT];
 #pragma unroll
         for (int r = 0; r < IPT; r++) {
-            uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
-            if (i < n) pol.pre(i, pre[r]);
+            const uint32_t li = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
+            if (li < cnt) pol.pre(base + li, pre[r]);
         }
 #pragma unroll
         for (int r = 0; r < IPT; r++) {
-            uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
+            const uint32_t li = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
             dg[r] = 256;
-            if (i < n) pol.load(i, pre[r], it[r], dg[r]);
+            if (li < cnt) pol.load(base + li, pre[r], it[r], dg[r]);
         }
     } else {
 #pragma unroll
         for (int r = 0; r < IPT; r++) {
-            uint64_t i = base + (uint64_t)w * 32 * IPT + (uint64_t)r * 32 + lane;
+            const uint32_t li = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
             dg[r] = 256;
-            if (i < n) pol.load(i, it[r], dg[r]);
+            if (li < cnt) pol.load(base + li, it[r], dg[r]);
         }
     }
     // stable ranks within the warp's sub-tile
@@ -186,12 +186,14 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
         s_wcnt[ww][d] = (uint16_t)count;
         count += c;
     }
-    s_tcount[d] = count;
-    s_excl[d] = os_lookback(status, tile, d, count, epoch, err);
+    const uint32_t excl = os_lookback(status, tile, d, count, epoch, err);
     uint32_t ex, tot;
     block_scan<uint32_t, OpSum<uint32_t>, OS_BLOCK>(count, OpSum<uint32_t>(), s_scan, &ex, &tot);
     s_tstart[d] = ex;
-    if (tile == ntiles - 1) pol.finish(d, s_excl[d] + count);
+    // the digit's item at tile position i has launch rank excl + i - ex
+    // (modular arithmetic: the true index is in range)
+    s_obase[d] = Policy::kOutSign > 0 ? pol.out0(d) + excl - ex : pol.out0(d) - excl + ex;
+    if (tile == ntiles - 1) pol.finish(d, excl + count);
     __syncthreads();
     // stage in digit order
 #pragma unroll
@@ -204,8 +206,8 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < tot; i += OS_BLOCK) {
-        uint32_t dd = s_dig[i];
-        uint64_t idx = pol.out(dd, (uint64_t)s_excl[dd] + (i - s_tstart[dd]));
+        const uint32_t dd = s_dig[i];
+        const uint64_t idx = Policy::kOutSign > 0 ? s_obase[dd] + i : s_obase[dd] - i;
         pol.store(idx, s_item[i], dd);
     }
 }
@@ -266,7 +268,8 @@ template <class Pred, class Emit> struct CompactPolicy {
             it = (uint32_t)i;
         }
     }
-    __device__ __forceinline__ uint64_t out(uint32_t, uint64_t r) const { return r; }
+    static constexpr int kOutSign = 1;
+    __device__ __forceinline__ uint64_t out0(uint32_t) const { return 0; }
     __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t) const { emit((uint64_t)it, (uint32_t)idx); }
     __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
         if (d == 0 && count) *count = total;

@@ -14,34 +14,6 @@ namespace psk {
 constexpr int RADIX_MAX_PASSES = 8;
 constexpr int RADIX_HIST_BLOCK = 256;
 
-template <class K, class V> struct RadixItem {
-    K k;
-    V v;
-};
-
-template <class K, class V> struct RadixPolicy {
-    using Item = RadixItem<K, V>;
-    static constexpr int kMinBlocks = sizeof(K) == 8 ? 3 : 4;
-    const K *kin;
-    const V *vin;
-    K *kout;
-    V *vout;
-    int shift;
-    uint32_t dmask;
-    const uint32_t *base;  // 256 digit bases of this pass
-    __device__ __forceinline__ void load(uint64_t i, Item &it, uint32_t &d) const {
-        it.k = kin[i];
-        it.v = vin[i];
-        d = (uint32_t)(it.k >> shift) & dmask;
-    }
-    __device__ __forceinline__ uint64_t out(uint32_t d, uint64_t r) const { return (uint64_t)base[d] + r; }
-    __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t) const {
-        kout[idx] = it.k;
-        vout[idx] = it.v;
-    }
-    __device__ __forceinline__ void finish(uint32_t, uint32_t) const {}
-};
-
 // One radix pass as a TMA-fed onesweep tile.  A full tile's keys and values
 // arrive in shared memory by two bulk copies on an mbarrier (the ragged last
 // tile, or unaligned arrays, use plain loads), so no item is held in a
