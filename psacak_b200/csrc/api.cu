@@ -279,6 +279,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     // Stage 2: name them and build the reduced string.
     DBuf<uint32_t> red, heads, flags, sa1, names1;
     DBuf<uint64_t> sorted_win;  // byte levels, bucket engine: final-mode LMS list with predecessor windows
+    DBuf<uint64_t> sorted_sym;  // doubling engine: final-mode LMS list with the positions' symbols
     uint32_t k = 0;
     if (n1 > 0 && !extracted) {
         PSK_TRY(ctx.compact(SortedLmsPred{sa, lms, n, ctx.d_err}, SortedLmsEmit{sa, sorted}, n, ctx.d_scalars + 1,
@@ -293,8 +294,10 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         PSK_TRY(red.init(ctx, n1));
         PSK_TRY(heads.init(ctx, n1 + 1));
         PSK_TRY(flags.init(ctx, n1));
-        PSK_TRY(name_lms<C>(text, n, lms, pref, sorted, n1, red, heads, flags, ctx.d_scalars + 2, env, ctx.scan_ctas,
-                            s));
+        DBuf<uint64_t> lmsx;
+        PSK_TRY(lmsx.init(ctx, nwords));
+        PSK_TRY(name_lms<C>(text, n, lms, pref, sorted, n1, red, heads, flags, lmsx, ctx.d_scalars + 2, env,
+                            ctx.scan_ctas, s));
         PSK_TRY(ctx.read_u32(ctx.d_scalars + 2, &k));
     }
     sorted.reset();
@@ -355,8 +358,15 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
                 PSK_TRY(permute_lms8(sa1, n1, text, lms, pref, n, plist, sorted_win, ctx.d_err, s));
             }
         }
-        // red is free again; reuse it as the position list of the permutation.
-        if (!sorted_win.get()) PSK_TRY(permute_lms(sa1, n1, lms, pref, n, red, ctx.d_err, s));
+        // the doubling scans take the list with the LMS positions' symbols
+        if (!sorted_win.get()) {
+            red.reset();
+            names1.reset();
+            DBuf<uint64_t> plist;
+            PSK_TRY(sorted_sym.init(ctx, n1));
+            PSK_TRY(plist.init(ctx, n1));
+            PSK_TRY(permute_lms_sym<C>(sa1, n1, text, lms, pref, n, plist, sorted_sym, ctx.d_err, s));
+        }
     } else {
         if (level == 0 && ctx.debug_red) {
             ctx.debug_n1 = 0;
@@ -375,9 +385,12 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
             sa1.reset();
             return induce_bucket8(ctx, text, n, lms, hg, dgeom.get(), INDUCE_FINAL, sorted_win, n1, sa, s);
         }
-        return induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
+        sa1.reset();
+        return induce_doubling<C>(ctx, text, n, types, lms, geom, 256, INDUCE_FINAL, sorted_sym, n1, nullptr, sa, s);
     } else {
-        return induce_doubling<C>(ctx, text, n, types, lms, geom, nbuckets, INDUCE_FINAL, sa1, n1, nullptr, sa, s);
+        sa1.reset();
+        return induce_doubling<C>(ctx, text, n, types, lms, geom, nbuckets, INDUCE_FINAL, sorted_sym, n1, nullptr, sa,
+                                  s);
     }
 }
 

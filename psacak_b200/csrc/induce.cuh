@@ -58,13 +58,14 @@ enum InduceMode { INDUCE_LMS_SUBSTRINGS = 0, INDUCE_FINAL = 1 };
 
 // Chain-doubling induced sort.  In INDUCE_LMS_SUBSTRINGS mode the LMS
 // positions start in arbitrary order at their bucket tails; in INDUCE_FINAL
-// mode `sorted_lms` (n1 entries, ascending suffix order) gives their order.
+// mode `sorted_lms` (n1 entries, ascending suffix order, each position |
+// its symbol << 32, permute_lms_sym) gives their order.
 // Writes every SA slot.  `cursor` is n (u32 levels) or 256 (byte levels)
 // zeroed uint32 used to place LMS positions in the first mode.
 // `nbuckets` = number of distinct symbols (dense ids 0..nbuckets-1).
 template <class C>
 status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
-                         Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
+                         Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint64_t *sorted_lms, uint64_t n1,
                          uint32_t *cursor, uint32_t *sa, cudaStream_t s);
 
 // Suffix array of a u32 level directly by prefix doubling (recursion finisher).

@@ -102,16 +102,16 @@ template <class C> struct LastLoad {
         uint32_t p;     // the LMS position
         uint32_t tail;  // tail slot (+1) of its bucket
     };
-    const C *text;
-    const uint32_t *sorted;
+    const uint64_t *sorted;  // position | symbol << 32, in suffix order
     uint64_t n1;
     Geom<C> g;
     __device__ __forceinline__ uint32_t operator()(uint64_t r, Payload &pl) const {
         uint64_t i = n1 - 1 - r;
-        pl.p = sorted[i];
-        const C c = text[pl.p];
+        const uint64_t e = sorted[i];
+        pl.p = (uint32_t)e;
+        const C c = (C)(e >> 32);
         pl.tail = g.tail(c);
-        bool last = (i + 1 == n1) || g.bucket(text[sorted[i + 1]]) != g.bucket(c);
+        bool last = (i + 1 == n1) || g.bucket((C)(sorted[i + 1] >> 32)) != g.bucket(c);
         return last ? (uint32_t)(r + 1) : 0u;
     }
 };
@@ -403,7 +403,7 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
 
 template <class C>
 status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *types, const uint32_t *lms,
-                         Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint32_t *sorted_lms, uint64_t n1,
+                         Geom<C> geom, uint64_t nbuckets, InduceMode mode, const uint64_t *sorted_lms, uint64_t n1,
                          uint32_t *cursor, uint32_t *sa, cudaStream_t s) {
     DBuf<uint32_t> R, v0, v1, gA, gB;
     DBuf<uint64_t> k0, k1;
@@ -426,7 +426,7 @@ status_t induce_doubling(Ctx &ctx, const C *text, uint64_t n, const uint32_t *ty
                                                                                             cursor, R)));
         PSK_LAUNCH_CHECK();
     } else if (n1 > 0) {
-        PSK_TRY((ctx.scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{text, sorted_lms, n1, geom},
+        PSK_TRY((ctx.scan<uint32_t, OpMax<uint32_t>>(LastLoad<C>{sorted_lms, n1, geom},
                                                      LastStore<C>{n1, R}, n1,
                                                      (uint32_t *)nullptr, OpMax<uint32_t>(), "scan_last")));
     }
@@ -462,10 +462,10 @@ status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bhead
 }
 
 template status_t induce_doubling<uint8_t>(Ctx &, const uint8_t *, uint64_t, const uint32_t *, const uint32_t *,
-                                           Geom<uint8_t>, uint64_t, InduceMode, const uint32_t *, uint64_t, uint32_t *,
+                                           Geom<uint8_t>, uint64_t, InduceMode, const uint64_t *, uint64_t, uint32_t *,
                                            uint32_t *, cudaStream_t);
 template status_t induce_doubling<uint32_t>(Ctx &, const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
-                                            Geom<uint32_t>, uint64_t, InduceMode, const uint32_t *, uint64_t,
+                                            Geom<uint32_t>, uint64_t, InduceMode, const uint64_t *, uint64_t,
                                             uint32_t *, uint32_t *, cudaStream_t);
 
 }  // namespace psk

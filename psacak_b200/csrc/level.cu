@@ -237,15 +237,25 @@ status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, u
 // next LMS position and the same characters; a substring that reaches the
 // end of the text contains the sentinel and equals nothing else.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t next_lms(const uint32_t *lms, uint64_t n, uint64_t p) {
+// lmsx[w] = lms[w] | pref[w] << 32: a word of the LMS bitmap beside the
+// number of LMS positions before it, so that one 8-byte read gives both the
+// next LMS position after p and the rank of p.
+__global__ void k_lms_pack(const uint32_t *__restrict__ lms, const uint32_t *__restrict__ pref, uint64_t nwords,
+                           uint64_t *lmsx) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x)
+        lmsx[w] = lms[w] | (uint64_t)pref[w] << 32;
+}
+
+// First LMS position after p (n if none); x0 = lmsx[p >> 5].
+__device__ __forceinline__ uint64_t next_lms(const uint64_t *lmsx, uint64_t n, uint64_t p, uint64_t x0) {
     uint64_t w = p >> 5;
     uint32_t sh = (uint32_t)(p & 31);
-    uint32_t word = sh == 31 ? 0u : (lms[w] & (FULL_MASK << (sh + 1)));
+    uint32_t word = sh == 31 ? 0u : ((uint32_t)x0 & (FULL_MASK << (sh + 1)));
     const uint64_t nwords = ceil_div(n, 32);
     while (!word) {
         w++;
         if (w >= nwords) return n;
-        word = lms[w];
+        word = (uint32_t)lmsx[w];
     }
     return (w << 5) + (uint64_t)(__ffs(word) - 1);
 }
@@ -263,9 +273,9 @@ template <class C> struct LmsFp {
     uint32_t w[4];  // first min(len + 1, W) characters
 };
 template <class C>
-__device__ __forceinline__ LmsFp<C> lms_fp(const C *text, uint64_t n, const uint32_t *lms, uint64_t p) {
+__device__ __forceinline__ LmsFp<C> lms_fp(const C *text, uint64_t n, const uint64_t *lmsx, uint64_t p, uint64_t x0) {
     LmsFp<C> f;
-    const uint64_t e = next_lms(lms, n, p);
+    const uint64_t e = next_lms(lmsx, n, p, x0);
     f.len = e >= n ? LmsFp<C>::END : (uint32_t)(e - p);
 #pragma unroll
     for (int i = 0; i < 4; i++) f.w[i] = 0;
@@ -287,11 +297,12 @@ __device__ __forceinline__ bool lms_fp_equal(const C *text, const LmsFp<C> &fa, 
     return true;
 }
 
-// flags[i] = 1 iff sorted LMS substring i differs from i - 1.  Each thread
+// flags[i] = (1 iff sorted LMS substring i differs from i - 1) << 31 | the
+// text-order rank of its LMS position (< n1 <= 2^31).  Each thread
 // fingerprints its own substring once and takes its neighbour's from the
 // lane below (lane 0 fingerprints its neighbour itself).
 template <class C>
-__global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint32_t *__restrict__ lms,
+__global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint64_t *__restrict__ lmsx,
                              const uint32_t *__restrict__ sorted, uint64_t n1, uint32_t *flags) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32
@@ -299,8 +310,9 @@ __global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint3
         const uint64_t i = ib + lane;
         const bool valid = i < n1;
         const uint64_t p = valid ? sorted[i] : 0;
+        const uint64_t x = valid ? lmsx[p >> 5] : 0ull;
         LmsFp<C> f;
-        if (valid) f = lms_fp(text, n, lms, p);
+        if (valid) f = lms_fp(text, n, lmsx, p, x);
         else f.len = LmsFp<C>::END;
         uint64_t q = __shfl_up_sync(FULL_MASK, p, 1);
         LmsFp<C> g;
@@ -312,27 +324,27 @@ __global__ void k_name_flags(const C *__restrict__ text, uint64_t n, const uint3
             if (i > 0) {
                 if (lane == 0) {
                     q = sorted[i - 1];
-                    g = lms_fp(text, n, lms, q);
+                    g = lms_fp(text, n, lmsx, q, lmsx[q >> 5]);
                 }
                 flag = lms_fp_equal(text, g, q, f, p) ? 0u : 1u;
             }
-            flags[i] = flag;
+            const uint32_t rank = (uint32_t)(x >> 32) + __popc((uint32_t)x & (uint32_t)((1ull << (p & 31)) - 1));
+            flags[i] = flag << 31 | rank;
         }
     }
 }
 
-// The load also finds the text-order rank of the LMS position (two gathers),
-// so that the store only writes.
+// The load takes the flag and the text-order rank of the LMS position that
+// k_name_flags packed together, so the scan reads one sequential word per
+// item and the store only writes.
 struct NameLoad {
     using Payload = uint32_t;  // rank of sorted[i] among the LMS positions
     static constexpr int kIPT = 8;
     const uint32_t *flags;
-    const uint32_t *sorted;
-    const uint32_t *lms;
-    const uint32_t *pref;
     __device__ __forceinline__ uint32_t operator()(uint64_t i, uint32_t &rank) const {
-        rank = lms_rank(lms, pref, sorted[i]);
-        return flags[i];
+        const uint32_t v = flags[i];
+        rank = v & 0x7FFFFFFFu;
+        return v >> 31;
     }
 };
 struct NameStore {
@@ -350,24 +362,28 @@ struct NameStore {
 template <class C>
 status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t *lms_pref,
                   const uint32_t *sorted, uint64_t n1, uint32_t *red, uint32_t *heads, uint32_t *flags,
-                  uint32_t *k_out, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s) {
+                  uint64_t *lmsx, uint32_t *k_out, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s) {
     if (n1 == 0) {
         PSK_CUDA(cudaMemsetAsync(k_out, 0, sizeof(uint32_t), s));
         return PSACAK_OK;
     }
+    const uint64_t nwords = ceil_div(n, 32);
+    const uint64_t gw = ceil_div(nwords, 256);
+    PSK_PROF_LAUNCH(s, "name_flags", nwords, 16 * nwords,
+                    (k_lms_pack<<<(uint32_t)(gw < 4096 ? gw : 4096), 256, 0, s>>>(lms, lms_pref, nwords, lmsx)));
     uint32_t grid = (uint32_t)(ceil_div(n1, 256) < (uint64_t)max_ctas * 4 ? ceil_div(n1, 256) : (uint64_t)max_ctas * 4);
-    PSK_PROF_LAUNCH(s, "name_flags", n1, 0, (k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lms, sorted, n1, flags)));
+    PSK_PROF_LAUNCH(s, "name_flags", n1, 0, (k_name_flags<C><<<grid, 256, 0, s>>>(text, n, lmsx, sorted, n1, flags)));
     PSK_LAUNCH_CHECK();
-    return lb_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags, sorted, lms, lms_pref}, NameStore{red, heads, n1}, n1,
-                                              k_out, OpSum<uint32_t>(), *env.ss, *env.os, env.err, s, "scan_names");
+    return lb_scan<uint32_t, OpSum<uint32_t>>(NameLoad{flags}, NameStore{red, heads, n1}, n1, k_out,
+                                              OpSum<uint32_t>(), *env.ss, *env.os, env.err, s, "scan_names");
 }
 
 template status_t name_lms<uint8_t>(const uint8_t *, uint64_t, const uint32_t *, const uint32_t *, const uint32_t *,
-                                    uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *, const ScanEnv &,
-                                    uint32_t, cudaStream_t);
+                                    uint64_t, uint32_t *, uint32_t *, uint32_t *, uint64_t *, uint32_t *,
+                                    const ScanEnv &, uint32_t, cudaStream_t);
 template status_t name_lms<uint32_t>(const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
-                                     const uint32_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *,
-                                     const ScanEnv &, uint32_t, cudaStream_t);
+                                     const uint32_t *, uint64_t, uint32_t *, uint32_t *, uint32_t *, uint64_t *,
+                                     uint32_t *, const ScanEnv &, uint32_t, cudaStream_t);
 
 __global__ void k_translate(uint32_t *red, uint64_t n1, const uint32_t *__restrict__ types,
                             const uint32_t *__restrict__ heads, uint32_t *err) {
@@ -403,53 +419,6 @@ status_t translate_names(uint32_t *red, uint64_t n1, const uint32_t *types, cons
     return PSACAK_OK;
 }
 
-// P[rank] = position for every LMS position.
-__global__ void k_lms_list(const uint32_t *__restrict__ lms, const uint32_t *__restrict__ pref, uint64_t nwords,
-                           uint32_t *plist) {
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t word = lms[w];
-        uint32_t o = pref[w];
-        while (word) {
-            int b = __ffs(word) - 1;
-            plist[o++] = (uint32_t)((w << 5) + b);
-            word &= word - 1;
-        }
-    }
-}
-
-__global__ void k_permute(uint32_t *sa1, uint64_t n1, const uint32_t *__restrict__ plist, uint32_t *err) {
-    constexpr int U = 4;  // entries per thread step: their gathers overlap
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n1; i0 += stride * U) {
-        uint32_t r[U], v[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) r[u] = i0 + u * stride < n1 ? sa1[i0 + u * stride] : 0u;
-#pragma unroll
-        for (int u = 0; u < U; u++) v[u] = r[u] < n1 ? plist[r[u]] : 0u;
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const uint64_t i = i0 + u * stride;
-            if (i >= n1) continue;
-            if (r[u] >= n1) dev_fail(err, DEVERR_RANGE);
-            sa1[i] = v[u];
-        }
-    }
-}
-
-status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint32_t *lms_pref, uint64_t n,
-                     uint32_t *plist, uint32_t *err, cudaStream_t s) {
-    if (n1 == 0) return PSACAK_OK;
-    uint64_t nwords = ceil_div(n, 32);
-    uint64_t g = ceil_div(nwords, 256);
-    k_lms_list<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(lms, lms_pref, nwords, plist);
-    PSK_KCOUNT();
-    g = ceil_div(n1, 256);
-    k_permute<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(sa1, n1, plist, err);
-    PSK_KCOUNT();
-    PSK_LAUNCH_CHECK();
-    return PSACAK_OK;
-}
-
 // Byte levels: the permuted list carries each LMS position's predecessor
 // window, p | win_fill(text, p) << 32, so that the final placement needs no
 // gather from the text.
@@ -467,8 +436,27 @@ __global__ void k_lms_list8(const uint8_t *__restrict__ text, const uint32_t *__
     }
 }
 
-__global__ void k_permute8(const uint32_t *__restrict__ sa1, uint64_t n1, const uint64_t *__restrict__ plist,
-                           uint64_t *out, uint32_t *err) {
+// Any level, doubling engine: the permuted list carries each LMS position's
+// symbol, p | text[p] << 32, so that the final placement (which compares the
+// symbols of neighbouring list entries) reads the list in order only.
+template <class C>
+__global__ void k_lms_list_sym(const C *__restrict__ text, const uint32_t *__restrict__ lms,
+                               const uint32_t *__restrict__ pref, uint64_t nwords, uint64_t *plist) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t word = lms[w];
+        uint32_t o = pref[w];
+        while (word) {
+            int b = __ffs(word) - 1;
+            const uint64_t p = (w << 5) + b;
+            plist[o++] = p | (uint64_t)(uint32_t)text[p] << 32;
+            word &= word - 1;
+        }
+    }
+}
+
+// out[i] = plist[sa1[i]] for 64-bit list entries.
+__global__ void k_permute_pairs(const uint32_t *__restrict__ sa1, uint64_t n1, const uint64_t *__restrict__ plist,
+                                uint64_t *out, uint32_t *err) {
     constexpr int U = 4;  // entries per thread step: their gathers overlap
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n1; i0 += stride * U) {
@@ -497,11 +485,31 @@ status_t permute_lms8(const uint32_t *sa1, uint64_t n1, const uint8_t *text, con
     k_lms_list8<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(text, lms, lms_pref, nwords, plist);
     PSK_KCOUNT();
     g = ceil_div(n1, 256);
-    k_permute8<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(sa1, n1, plist, out, err);
+    k_permute_pairs<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(sa1, n1, plist, out, err);
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
+
+template <class C>
+status_t permute_lms_sym(const uint32_t *sa1, uint64_t n1, const C *text, const uint32_t *lms, const uint32_t *lms_pref,
+                         uint64_t n, uint64_t *plist, uint64_t *out, uint32_t *err, cudaStream_t s) {
+    if (n1 == 0) return PSACAK_OK;
+    uint64_t nwords = ceil_div(n, 32);
+    uint64_t g = ceil_div(nwords, 256);
+    k_lms_list_sym<C><<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(text, lms, lms_pref, nwords, plist);
+    PSK_KCOUNT();
+    g = ceil_div(n1, 256);
+    k_permute_pairs<<<(uint32_t)(g < 8192 ? g : 8192), 256, 0, s>>>(sa1, n1, plist, out, err);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+template status_t permute_lms_sym<uint8_t>(const uint32_t *, uint64_t, const uint8_t *, const uint32_t *,
+                                           const uint32_t *, uint64_t, uint64_t *, uint64_t *, uint32_t *, cudaStream_t);
+template status_t permute_lms_sym<uint32_t>(const uint32_t *, uint64_t, const uint32_t *, const uint32_t *,
+                                            const uint32_t *, uint64_t, uint64_t *, uint64_t *, uint32_t *,
+                                            cudaStream_t);
 
 __global__ void k_direct_inverse(const uint32_t *__restrict__ red, uint64_t n1, uint32_t *sa1, uint32_t *err) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += (uint64_t)gridDim.x * blockDim.x) {

@@ -42,33 +42,21 @@ status_t type_text(const C *text, uint64_t n, uint32_t *types, uint32_t *lms, ui
 status_t lms_prefix(const uint32_t *lms_wcnt, uint64_t nwords, uint32_t *pref, uint32_t *total,
                     const ScanEnv &env, cudaStream_t s);
 
-// Rank of LMS position p among LMS positions (number of LMS before p).
-__device__ __forceinline__ uint32_t lms_rank(const uint32_t *lms, const uint32_t *pref, uint64_t p) {
-    uint32_t w = lms[p >> 5];
-    uint32_t below = (uint32_t)((1ull << (p & 31)) - 1);
-    return pref[p >> 5] + __popc(w & below);
-}
-
 // Names the n1 sorted LMS substrings `sorted` (positions in `text`) and
-// builds the reduced string: red[rank(p)] = name.  diff/name scratch of n1.
-// heads[c] = index in `sorted` where name c starts (k entries, then n1).
-// *k_out (device) = number of names.
+// builds the reduced string: red[rank(p)] = name.  `flags` is scratch of n1
+// words, `lmsx` of ceil(n / 32) 64-bit words.  heads[c] = index in `sorted`
+// where name c starts (k entries, then n1).  *k_out (device) = number of
+// names.
 template <class C>
 status_t name_lms(const C *text, uint64_t n, const uint32_t *lms, const uint32_t *lms_pref,
                   const uint32_t *sorted, uint64_t n1, uint32_t *red, uint32_t *heads, uint32_t *flags,
-                  uint32_t *k_out, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s);
+                  uint64_t *lmsx, uint32_t *k_out, const ScanEnv &env, uint32_t max_ctas, cudaStream_t s);
 
 // Translates names in `red` (types in `types`) into bucket pointers in place:
 // L -> heads[c], S -> heads[c+1] - 1 (the reference's translate,
 // src/naming.rs:263-274).  heads has k+1 entries (heads[k] = n1).
 status_t translate_names(uint32_t *red, uint64_t n1, const uint32_t *types, const uint32_t *heads,
                          uint32_t *err, cudaStream_t s);
-
-// sa1[i] = P[sa1[i]] where P lists the LMS positions of `lms` in text order
-// (the reference's permutate_lmssuffixes, src/naming.rs:413-430).  `plist`
-// is scratch of n1 entries.
-status_t permute_lms(uint32_t *sa1, uint64_t n1, const uint32_t *lms, const uint32_t *lms_pref, uint64_t n,
-                     uint32_t *plist, uint32_t *err, cudaStream_t s);
 
 // Predecessor window of a byte-level SA entry x > 0, kept beside the entry
 // by the bucket scans: byte 0 = text[x-1] (the character that decides
@@ -105,6 +93,14 @@ __device__ __forceinline__ uint32_t run_win(uint32_t d, uint32_t r, uint32_t c, 
 status_t permute_lms8(const uint32_t *sa1, uint64_t n1, const uint8_t *text, const uint32_t *lms,
                       const uint32_t *lms_pref, uint64_t n, uint64_t *plist, uint64_t *out, uint32_t *err,
                       cudaStream_t s);
+
+// Any level: out[i] = P[sa1[i]] | text[P[sa1[i]]] << 32 where P lists the
+// LMS positions of `lms` in text order (the reference's
+// permutate_lmssuffixes, src/naming.rs:413-430), with the positions'
+// symbols.  `plist` is scratch of n1 entries.
+template <class C>
+status_t permute_lms_sym(const uint32_t *sa1, uint64_t n1, const C *text, const uint32_t *lms, const uint32_t *lms_pref,
+                         uint64_t n, uint64_t *plist, uint64_t *out, uint32_t *err, cudaStream_t s);
 
 // Direct inverse when all names are unique: sa1[red[i]] = i.
 status_t direct_inverse(const uint32_t *red, uint64_t n1, uint32_t *sa1, uint32_t *err, cudaStream_t s);
