@@ -23,6 +23,45 @@ constexpr int RADIX_HIST_BLOCK = 256;
 // of whole items: the scatter reads s_perm[i] and copies that item to
 // digit base + i, so consecutive threads write consecutive slots of a digit.
 // Shared memory: TILE * (sizeof(K) + sizeof(V) + 2) + 6.3 KB.
+// Stable ranks of the warp's IPT x 32 items of the tile (item idx = warp *
+// 32 * IPT + r * 32 + lane) by the digit (key >> shift) & dmask: rd[r] =
+// rank within the warp << 9 | digit (256 = no item); wcnt = the warp's digit
+// counters.  FULL: all TILE items are present (no validity tests).
+template <class K, int IPT, bool FULL>
+__device__ __forceinline__ void radix_rank(const K *s_k, uint32_t cnt, int shift, uint32_t dmask, uint16_t *wcnt,
+                                           uint32_t (&rd)[IPT]) {
+    const int w = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        const uint32_t idx = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
+        const bool valid = FULL || idx < cnt;
+        // the digit lies in one 32-bit half of the key (shift is a multiple of 8)
+        const uint32_t half = sizeof(K) == 8 ? reinterpret_cast<const uint32_t *>(s_k)[2 * idx + (shift >> 5)]
+                                             : (uint32_t)s_k[idx];
+        const uint32_t d = valid ? (half >> (shift & 31)) & dmask : 256u;
+        // lanes with the same digit: the intersection of eight bit ballots
+        // (ALU votes instead of one match.any through the MIO pipe)
+        uint32_t peers = FULL_MASK;
+        if (!FULL) {
+            peers = __ballot_sync(FULL_MASK, valid);
+            if (!valid) peers = ~peers;
+        }
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const uint32_t bit = (d >> b) & 1u;
+            const uint32_t bb = __ballot_sync(FULL_MASK, bit);
+            peers &= bit ? bb : ~bb;
+        }
+        const uint32_t prior = (FULL || d < 256) ? wcnt[d] : 0u;
+        rd[r] = ((prior + __popc(peers & lt)) << 9) | d;
+        __syncwarp();
+        if ((FULL || d < 256) && (int)lane == __ffs(peers) - 1) wcnt[d] = (uint16_t)(prior + __popc(peers));
+        __syncwarp();
+    }
+}
+
 constexpr int RS_MIN_BLOCKS = 4;
 constexpr int RADIX_IPT = 12;  // items per thread of the radix passes (3072-item tiles)
 
@@ -45,7 +84,6 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
 
     const int w = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t lt = lanemask_lt();
 
     if (threadIdx.x == 0) {
         s_tile = atomicAdd(ticket, 1u);
@@ -77,30 +115,8 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
 
     // stable ranks within the warp's sub-tile; packed (rank << 9 | digit)
     uint32_t rd[IPT];
-#pragma unroll
-    for (int r = 0; r < IPT; r++) {
-        const uint32_t idx = (uint32_t)w * 32 * IPT + (uint32_t)r * 32 + lane;
-        const bool valid = idx < cnt;
-        // the digit lies in one 32-bit half of the key (shift is a multiple of 8)
-        const uint32_t half = sizeof(K) == 8 ? reinterpret_cast<const uint32_t *>(s_k)[2 * idx + (shift >> 5)]
-                                             : (uint32_t)s_k[idx];
-        const uint32_t d = valid ? (half >> (shift & 31)) & dmask : 256u;
-        // lanes with the same digit: the intersection of eight bit ballots
-        // (ALU votes instead of one match.any through the MIO pipe)
-        uint32_t peers = __ballot_sync(FULL_MASK, valid);
-        if (!valid) peers = ~peers;
-#pragma unroll
-        for (int b = 0; b < 8; b++) {
-            const uint32_t bit = (d >> b) & 1u;
-            const uint32_t bb = __ballot_sync(FULL_MASK, bit);
-            peers &= bit ? bb : ~bb;
-        }
-        const uint32_t prior = d < 256 ? s_wcnt[w][d] : 0u;
-        rd[r] = ((prior + __popc(peers & lt)) << 9) | d;
-        __syncwarp();
-        if (d < 256 && (int)lane == __ffs(peers) - 1) s_wcnt[w][d] = (uint16_t)(prior + __popc(peers));
-        __syncwarp();
-    }
+    if (cnt == (uint32_t)TILE) radix_rank<K, IPT, true>(s_k, cnt, shift, dmask, s_wcnt[w], rd);
+    else radix_rank<K, IPT, false>(s_k, cnt, shift, dmask, s_wcnt[w], rd);
     __syncthreads();
     const uint32_t d = threadIdx.x;  // this thread's digit from here on
     uint32_t count = 0;
@@ -125,11 +141,14 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
         }
     }
     __syncthreads();
+    // n < 2^32 items: 32-bit output slots
+    const uint32_t n32 = (uint32_t)n;
     for (uint32_t i = threadIdx.x; i < cnt; i += OS_BLOCK) {
         const uint32_t li = s_perm[i];
         const K k = s_k[li];
-        const uint64_t o = (uint64_t)s_gbase[(uint32_t)(k >> shift) & dmask] + i;
-        if (o < n) {
+        const uint32_t half = sizeof(K) == 8 ? (uint32_t)(shift >= 32 ? (uint64_t)k >> 32 : (uint64_t)k) : (uint32_t)k;
+        const uint32_t o = s_gbase[(half >> (shift & 31)) & dmask] + i;
+        if (o < n32) {
             kout[o] = k;
             vout[o] = s_v[li];
         } else {
