@@ -672,6 +672,11 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     return PSACAK_OK;
 }
 
+// Pageable outputs at least this long are drained during the final scans
+// (shorter ones are copied after the build, where a host thread would cost
+// more than it hides).
+constexpr uint64_t PAGEABLE_SINK_MIN = 32ull << 20;
+
 template <class C>
 status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_schedule *sched) {
     PSK_CUDA(cudaSetDevice(c.dev.id));
@@ -692,10 +697,16 @@ status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_
     // make each of those copies wait for itself on the host, so it is filled
     // through the staging ring after the build.
     const bool out_pinned = n && host_is_pinned(sa);
-    bool sink = false;
-    if (sizeof(C) == 1 && out_pinned) {
+    bool sink = false, drain = false;
+    if (sizeof(C) == 1 && n && (out_pinned || n >= PAGEABLE_SINK_MIN)) {
         if (!c.copy_stream) PSK_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
         if (!c.copy_ev) PSK_CUDA(cudaEventCreateWithFlags(&c.copy_ev, cudaEventDisableTiming));
+        if (!out_pinned) {
+            // pageable: a host thread drains the parts through the staging ring
+            PSK_TRY(drain_begin(c, sa, ds.get()));
+            c.sink_pageable = true;
+            drain = true;
+        }
         c.sink_dev = ds.get();
         c.sink_host = sa;
         sink = true;
@@ -703,8 +714,11 @@ status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_
     c.sink_done = false;
     const status_t st = run_dev<C>(c, dt.get(), n, ds.get(), c.own_stream, sched);
     c.sink_dev = c.sink_host = nullptr;
+    c.sink_pageable = false;
+    const status_t dst = drain ? drain_end(c) : PSACAK_OK;
     if (sink) PSK_CUDA(cudaStreamSynchronize(c.copy_stream));  // before ds goes back to the arena
     PSK_TRY(st);
+    PSK_TRY(dst);
     if (n && !c.sink_done) {
         if (out_pinned)
             PSK_CUDA(cudaMemcpyAsync(sa, ds.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <vector>
 
+#include "hostio.cuh"
 #include "level.cuh"
 #include "radix.cuh"
 
@@ -53,11 +54,13 @@ struct Ctx {
     // build.  sink_done tells the caller that every slot was sent.
     uint32_t *sink_dev = nullptr, *sink_host = nullptr;
     bool sink_done = false;
+    bool sink_pageable = false;  // pageable destination: parts go to the drain thread (hostio.cuh)
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev = nullptr;
     HostStage *stage = nullptr;  // pageable host transfers (hostio.cuh), created on first use
     status_t sink_part(uint64_t first, uint64_t count) {
         if (count == 0) return PSACAK_OK;
+        if (sink_pageable) return drain_part(*this, first, count);
         PSK_CUDA(cudaEventRecord(copy_ev, stream));
         PSK_CUDA(cudaStreamWaitEvent(copy_stream, copy_ev, 0));
         PSK_CUDA(cudaMemcpyAsync(sink_host + first, sink_dev + first, count * sizeof(uint32_t),

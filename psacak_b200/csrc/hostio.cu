@@ -1,6 +1,7 @@
 // hostio.cu -- staged transfers of pageable host memory (see hostio.cuh).
 #include "hostio.cuh"
 
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -94,6 +95,22 @@ struct HostStage {
     char *ring = nullptr;  // two pinned slots of STAGE_CHUNK bytes
     cudaEvent_t ev[2] = {nullptr, nullptr};
     CopyPool *pool = nullptr;
+    // drain session (pageable sink)
+    struct Part {
+        uint64_t first, count;
+        cudaEvent_t ready;
+    };
+    std::thread drainer;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<Part> parts;           // handed over, not yet taken
+    std::vector<cudaEvent_t> part_ev;  // one per part of a session, reused across sessions
+    size_t nparts = 0;                 // parts of the current session
+    bool closing = false;
+    status_t status = PSACAK_OK;
+    char err[256] = "";
+    uint32_t *host = nullptr;
+    const uint32_t *dev = nullptr;
 };
 
 bool host_is_pinned(const void *p) {
@@ -200,9 +217,128 @@ status_t staged_download(Ctx &c, const char *d_src, const std::vector<HostPiece>
     return PSACAK_OK;
 }
 
+// The drain thread: every part waits for its event on the copy stream and
+// goes through the two ring slots, the DMA of one slot overlapping the host
+// copy of the other.
+static void drain_loop(Ctx *cp) {
+    Ctx &c = *cp;
+    HostStage &st = *c.stage;
+    cudaSetDevice(c.dev.id);
+    auto fail = [&](cudaError_t e, const char *what) {
+        std::lock_guard<std::mutex> g(st.mu);
+        if (st.status == PSACAK_OK) {
+            st.status = PSACAK_ECUDA;
+            snprintf(st.err, sizeof(st.err), "output copy: %s failed: %s", what, cudaGetErrorString(e));
+        }
+    };
+    std::vector<CopyTask> tasks;
+    uint64_t k = 0;  // pieces issued, for the slot alternation
+    for (;;) {
+        HostStage::Part part;
+        {
+            std::unique_lock<std::mutex> lk(st.mu);
+            st.cv.wait(lk, [&] { return st.closing || !st.parts.empty(); });
+            if (st.parts.empty()) return;  // closing and nothing left
+            part = st.parts.front();
+            st.parts.erase(st.parts.begin());
+        }
+        cudaError_t e = cudaStreamWaitEvent(c.copy_stream, part.ready, 0);
+        if (e != cudaSuccess) {
+            fail(e, "cudaStreamWaitEvent");
+            continue;
+        }
+        const uint64_t bytes = part.count * sizeof(uint32_t);
+        const char *src = (const char *)(st.dev + part.first);
+        char *dst = (char *)(st.host + part.first);
+        // pieces of one part: piece j + 1 is issued before piece j is copied out
+        int prev_slot = -1;
+        uint64_t prev_off = 0, prev_len = 0;
+        for (uint64_t off = 0;; off += STAGE_CHUNK) {
+            const bool more = off < bytes;
+            int slot = -1;
+            uint64_t len = 0;
+            if (more) {
+                slot = (int)(k++ & 1);
+                len = std::min(STAGE_CHUNK, bytes - off);
+                e = cudaMemcpyAsync(st.ring + slot * STAGE_CHUNK, src + off, len, cudaMemcpyDeviceToHost,
+                                    c.copy_stream);
+                if (e == cudaSuccess) e = cudaEventRecord(st.ev[slot], c.copy_stream);
+                if (e != cudaSuccess) {
+                    fail(e, "cudaMemcpyAsync");
+                    break;
+                }
+            }
+            if (prev_slot >= 0) {
+                e = cudaEventSynchronize(st.ev[prev_slot]);
+                if (e != cudaSuccess) {
+                    fail(e, "cudaEventSynchronize");
+                    break;
+                }
+                tasks.clear();
+                for (uint64_t x = 0; x < prev_len; x += COPY_TASK)
+                    tasks.push_back(CopyTask{dst + prev_off + x, st.ring + prev_slot * STAGE_CHUNK + x,
+                                             std::min(COPY_TASK, prev_len - x)});
+                st.pool->run(tasks);
+            }
+            if (!more) break;
+            prev_slot = slot;
+            prev_off = off;
+            prev_len = len;
+        }
+    }
+}
+
+status_t drain_begin(Ctx &c, uint32_t *host, const uint32_t *dev) {
+    PSK_TRY(stage_ready(c));
+    HostStage &st = *c.stage;
+    st.host = host;
+    st.dev = dev;
+    st.parts.clear();
+    st.nparts = 0;
+    st.closing = false;
+    st.status = PSACAK_OK;
+    st.err[0] = 0;
+    st.drainer = std::thread(drain_loop, &c);
+    return PSACAK_OK;
+}
+
+status_t drain_part(Ctx &c, uint64_t first, uint64_t count) {
+    if (count == 0) return PSACAK_OK;
+    HostStage &st = *c.stage;
+    if (st.nparts == st.part_ev.size()) {
+        cudaEvent_t e;
+        PSK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        st.part_ev.push_back(e);
+    }
+    cudaEvent_t ev = st.part_ev[st.nparts++];
+    PSK_CUDA(cudaEventRecord(ev, c.stream));
+    {
+        std::lock_guard<std::mutex> g(st.mu);
+        st.parts.push_back(HostStage::Part{first, count, ev});
+    }
+    st.cv.notify_one();
+    return PSACAK_OK;
+}
+
+status_t drain_end(Ctx &c) {
+    HostStage &st = *c.stage;
+    {
+        std::lock_guard<std::mutex> g(st.mu);
+        st.closing = true;
+    }
+    st.cv.notify_one();
+    if (st.drainer.joinable()) st.drainer.join();
+    PSK_CUDA(cudaStreamSynchronize(c.copy_stream));
+    if (st.status != PSACAK_OK) return set_error(st.status, "%s", st.err);
+    return PSACAK_OK;
+}
+
 void host_stage_free(Ctx &c) {
     if (!c.stage) return;
     HostStage &st = *c.stage;
+    if (st.drainer.joinable()) drain_end(c);
+    for (cudaEvent_t e : st.part_ev) cudaEventDestroy(e);
+    st.part_ev.clear();
     for (int i = 0; i < 2; i++)
         if (st.ev[i]) {
             cudaEventSynchronize(st.ev[i]);

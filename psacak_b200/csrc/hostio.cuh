@@ -36,6 +36,16 @@ status_t staged_upload(Ctx &c, char *d_dst, const std::vector<HostPiece> &pieces
 // already queued on `s`; returns when the host ranges hold the data.
 status_t staged_download(Ctx &c, const char *d_src, const std::vector<HostPiece> &pieces, cudaStream_t s);
 
+// Pageable destination of the final suffix array (see Ctx::sink_part): a
+// host thread takes each finished part, moves it through the staging ring
+// and copies it into `host` while the build goes on.  drain_begin starts the
+// thread, drain_part (build thread, after the part's kernels are queued on
+// the build stream) hands it a part, drain_end waits for every part and
+// returns the first failure.
+status_t drain_begin(Ctx &c, uint32_t *host, const uint32_t *dev);
+status_t drain_part(Ctx &c, uint64_t first, uint64_t count);
+status_t drain_end(Ctx &c);
+
 // Releases the context's staging ring and host threads.
 void host_stage_free(Ctx &c);
 

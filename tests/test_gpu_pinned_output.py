@@ -93,3 +93,20 @@ def test_batch_with_pageable_and_pinned_buffers():
         assert (got[i] == outs[i]).all(), i
     for i in (1, 5, 50, 199):
         assert (got[i] == o.psacak8(texts[i])).all(), i
+
+
+def test_pageable_output_drained_during_the_scans():
+    """Pageable outputs of 32M symbols and more are drained by a host thread
+    while the final scans run; many small bucket parts (random bytes: 512
+    parts) and a single bucket (one byte value) both arrive intact."""
+    rng = np.random.default_rng(13)
+    for t in (rng.integers(0, 256, 40_000_000).astype(np.uint8), np.full(34_000_000, 7, np.uint8)):
+        page = np.empty(t.size, np.uint32)
+        pk.psacak_inplace(t, page)
+        pin = pinned_u32(t.size)
+        pk.psacak_inplace(t, pin)
+        assert (page == pin).all()
+        with pk.Context(0) as ctx:
+            dt = torch.from_numpy(t).cuda()
+            ds = torch.from_numpy(page.view(np.int32)).cuda()
+            assert ctx.check_sa8_dev(dt.data_ptr(), t.size, ds.data_ptr())
