@@ -81,6 +81,21 @@ PSACAK_API const char *psacak_last_error_string(void);
 PSACAK_API const char *psacak_version(void);
 
 /*
+ * psacak_init -- makes `device` the device of the calling thread's default
+ * context (the one psacak8 / psacak32 use) and creates that context now, so
+ * that the first build does not pay for CUDA start-up, the pinned buffers
+ * and the helper threads.  Optional: without it the default context is
+ * created on device 0 by the first build.  PSACAK_EINVAL for a device that
+ * does not exist.
+ * psacak_shutdown -- releases the calling thread's default context (device
+ * workspace, pinned buffers, host copy threads).  A later psacak8 / psacak32
+ * call creates a new one.  The reference has neither: its calls keep no state
+ * between them (src/lib.rs:64-82).
+ */
+PSACAK_API int psacak_init(int device);
+PSACAK_API int psacak_shutdown(void);
+
+/*
  * psacak8 -- suffix array of a byte string, host pointers.
  * Replaces psacak_inplace(text: &[u8], suf: &mut [u32]) (src/lib.rs:77-82)
  * and psacak (src/lib.rs:64-69), which drive psacak8 (src/psacak8.rs:19).

@@ -110,6 +110,7 @@ def lib():
         L.psacak_last_error_string.restype = ctypes.c_char_p
         L.psacak_version.restype = ctypes.c_char_p
         L.psacak8.argtypes = [p, u64, p]
+        L.psacak_init.argtypes = [i32]
         L.psacak32.argtypes = [p, u64, p]
         L.psacak8_ctx.argtypes = [p, p, u64, p, p]
         L.psacak32_ctx.argtypes = [p, p, u64, p, p]
@@ -327,6 +328,26 @@ def _ctx():
         c = Context(0)
         _default.ctx = c
     return c
+
+
+def init(device=0):
+    """Creates the calling thread's default C-ABI context on `device` now
+    (psacak_init) and makes the Python default context use that device too."""
+    _raise(lib().psacak_init(int(device)))
+    c = getattr(_default, "ctx", None)
+    if c is not None:
+        c.close()
+    _default.ctx = Context(int(device))
+
+
+def shutdown():
+    """Releases the calling thread's default contexts (psacak_shutdown); the
+    next build creates new ones."""
+    c = getattr(_default, "ctx", None)
+    if c is not None:
+        c.close()
+        _default.ctx = None
+    _raise(lib().psacak_shutdown())
 
 
 def psacak(text):

@@ -737,10 +737,11 @@ status_t run_host(Ctx &c, const C *text, uint64_t n, uint32_t *sa, const psacak_
 using namespace psk;
 
 static thread_local psacak_ctx *t_default_ctx = nullptr;
+static thread_local int t_default_device = 0;
 
 static int default_ctx(psacak_ctx **out) {
     if (!t_default_ctx) {
-        int rc = psacak_ctx_create(0, &t_default_ctx);
+        int rc = psacak_ctx_create(t_default_device, &t_default_ctx);
         if (rc != PSACAK_OK) return rc;
     }
     *out = t_default_ctx;
@@ -750,6 +751,28 @@ static int default_ctx(psacak_ctx **out) {
 extern "C" {
 
 const char *psacak_version(void) { return "0.1.0"; }
+
+int psacak_init(int device) {
+    clear_error();
+    if (device < 0) return set_error(PSACAK_EINVAL, "psacak_init: device %d", device);
+    int count = 0;
+    PSK_CUDA(cudaGetDeviceCount(&count));
+    if (device >= count) return set_error(PSACAK_EINVAL, "psacak_init: device %d of %d", device, count);
+    if (t_default_ctx && t_default_ctx->c.dev.id != device) {
+        psacak_ctx_destroy(t_default_ctx);
+        t_default_ctx = nullptr;
+    }
+    t_default_device = device;
+    psacak_ctx *c = nullptr;
+    return default_ctx(&c);
+}
+
+int psacak_shutdown(void) {
+    clear_error();
+    if (t_default_ctx) psacak_ctx_destroy(t_default_ctx);
+    t_default_ctx = nullptr;
+    return PSACAK_OK;
+}
 
 const char *psacak_last_error_string(void) { return last_error(); }
 

@@ -65,3 +65,9 @@ def test_python_limits_raise():
         pk.psacak_inplace(b"abc", np.zeros(2, np.uint32))
     with pytest.raises(TypeError):
         pk.psacak_inplace(b"abc", np.zeros(3, np.int64))
+
+
+def test_init_rejects_bad_devices_and_shutdown_without_context():
+    lib = pk.lib()
+    assert lib.psacak_init(-1) == pk.PSACAK_EINVAL
+    assert lib.psacak_shutdown() == 0

@@ -157,3 +157,23 @@ def test_byte_texts_sorted_directly_by_prefix_doubling(ctx, finish):
     for t in texts:
         sc = {"engine": pk.ENGINE_BUCKET, "inner_engine": pk.ENGINE_DOUBLING, "finish_below": finish}
         assert (ctx.psacak(t, sc) == o.psacak8(t)).all(), (finish, t.size)
+
+
+def test_init_and_shutdown_of_the_default_context():
+    """psacak_init creates the thread's default context up front; after
+    psacak_shutdown the next call creates a new one and builds the same SA."""
+    t = synth.genome(200_000, seed=31)
+    want = o.psacak8(t)
+    pk.init(0)
+    assert (pk.psacak(t) == want).all()
+    import ctypes
+    sa = np.empty(t.size, np.uint32)
+    assert pk.lib().psacak8(ctypes.c_void_p(t.ctypes.data), t.size, ctypes.c_void_p(sa.ctypes.data)) == 0
+    assert (sa == want).all()
+    pk.shutdown()
+    sa[:] = 0
+    assert pk.lib().psacak8(ctypes.c_void_p(t.ctypes.data), t.size, ctypes.c_void_p(sa.ctypes.data)) == 0
+    assert (sa == want).all()
+    assert (pk.psacak(t) == want).all()
+    bad = pk.lib().psacak_init(1 << 20)
+    assert bad == -1
