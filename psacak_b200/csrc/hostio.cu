@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <exception>
 #include <mutex>
+#include <new>
 #include <thread>
 
 #include "ctx.cuh"
@@ -30,8 +32,16 @@ struct CopyTask {
 // the calling thread works on the list too.
 class CopyPool {
   public:
+    // Starts up to `workers` threads; if the system refuses one, the pool
+    // works with those it has (the calling thread always takes part).
     explicit CopyPool(unsigned workers) {
-        for (unsigned i = 0; i < workers; i++) threads_.emplace_back([this] { loop(); });
+        for (unsigned i = 0; i < workers; i++) {
+            try {
+                threads_.emplace_back([this] { loop(); });
+            } catch (const std::exception &) {
+                break;
+            }
+        }
     }
     ~CopyPool() {
         {
@@ -121,7 +131,8 @@ bool host_is_pinned(const void *p) {
 }
 
 static status_t stage_ready(Ctx &c) {
-    if (!c.stage) c.stage = new HostStage();
+    if (!c.stage) c.stage = new (std::nothrow) HostStage();
+    if (!c.stage) return set_error(PSACAK_ENOMEM, "staging: out of host memory");
     HostStage &st = *c.stage;
     if (!st.ring) PSK_CUDA(cudaHostAlloc((void **)&st.ring, 2 * STAGE_CHUNK, cudaHostAllocDefault));
     for (int i = 0; i < 2; i++)
@@ -129,7 +140,8 @@ static status_t stage_ready(Ctx &c) {
     if (!st.pool) {
         unsigned hw = std::thread::hardware_concurrency();
         unsigned t = std::min(hw ? hw : 1u, MAX_COPY_THREADS);
-        st.pool = new CopyPool(t - 1);
+        st.pool = new (std::nothrow) CopyPool(t - 1);
+        if (!st.pool) return set_error(PSACAK_ENOMEM, "staging: out of host memory");
     }
     // the slots are free once the transfers of an earlier call have ended
     for (int i = 0; i < 2; i++) PSK_CUDA(cudaEventSynchronize(st.ev[i]));
@@ -298,7 +310,11 @@ status_t drain_begin(Ctx &c, uint32_t *host, const uint32_t *dev) {
     st.closing = false;
     st.status = PSACAK_OK;
     st.err[0] = 0;
-    st.drainer = std::thread(drain_loop, &c);
+    try {
+        st.drainer = std::thread(drain_loop, &c);
+    } catch (const std::exception &e) {
+        return set_error(PSACAK_ENOMEM, "output copy thread: %s", e.what());
+    }
     return PSACAK_OK;
 }
 
