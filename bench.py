@@ -66,7 +66,7 @@ def parse():
                          "zipf32 (psacak32 on 256M Zipf symbols), iid8m (8 MiB i.i.d. ACGT)")
     ap.add_argument("--requests", type=int, default=20000, help="serve: number of requests")
     ap.add_argument("--load", type=float, default=0.7, help="serve: arrival rate / measured capacity")
-    ap.add_argument("--regret-sample", type=int, default=200, help="serve: requests judged by exhaustive autotune")
+    ap.add_argument("--regret-sample", type=int, default=200, help="serve: requests whose selector choice is checked against exhaustive autotune")
     ap.add_argument("--plain-texts", type=int, default=0,
                     help="batch4096: time the per-text loop on this many texts (0 = all)")
     ap.add_argument("--single-build", action="store_true",

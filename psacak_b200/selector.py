@@ -6,7 +6,7 @@
   builds the same suffix array.
 * ``features`` -- 16 text statistics computed on the GPU (psacak_text_stats).
 * ``autotune`` -- exhaustive search: times every schedule on a text.  It is
-  the fallback when no trained model is available and the judge of the
+  the fallback when no trained model is available and the yardstick for the
   model's picks (regret = picked time / best time - 1).
 * ``Selector`` -- fp32 MLP 16 -> 64 -> 64 -> K predicting log2(ms) of every
   schedule; trained on the GPU by the library's own forward / backward / Adam

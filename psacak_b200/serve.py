@@ -84,7 +84,7 @@ def run(ctx, net, count=20000, seed=5, load=0.7, autotune_sample=200, lo=4 << 10
         "throughput_suffixes_per_s": symbols / makespan, "total_suffixes": symbols,
         "schedule_histogram": {str(k): int((picks == k).sum()) for k in range(len(sel.SCHEDULES))},
     }
-    # regret on a sample, judged by exhaustive autotuning
+    # regret on a sample, measured against exhaustive autotuning
     if autotune_sample:
         idx = np.random.default_rng(seed + 11).choice(count, min(autotune_sample, count), replace=False)
         reg_sel, reg_def = [], []
