@@ -61,9 +61,10 @@ def parse():
     ap.add_argument("--engine", type=int, default=0, help="psacak_schedule.engine (0 = auto)")
     ap.add_argument("--profile-json", default="", help="also write per-kernel stats here")
     ap.add_argument("--workload", default="genome1g",
-                    choices=["genome1g", "batch4096", "zipf32", "iid8m", "serve", "derived"],
+                    choices=["genome1g", "batch4096", "zipf32", "iid8m", "serve", "derived", "short20k"],
                     help="genome1g (default, the headline), batch4096 (4096 texts in one batched build), "
-                         "zipf32 (psacak32 on 256M Zipf symbols), iid8m (8 MiB i.i.d. ACGT)")
+                         "zipf32 (psacak32 on 256M Zipf symbols), iid8m (8 MiB i.i.d. ACGT), "
+                         "short20k (20,000 texts of 256 B..8 KiB in one batched build)")
     ap.add_argument("--requests", type=int, default=20000, help="serve: number of requests")
     ap.add_argument("--load", type=float, default=0.7, help="serve: arrival rate / measured capacity")
     ap.add_argument("--regret-sample", type=int, default=200, help="serve: requests whose selector choice is checked against exhaustive autotune")
@@ -75,6 +76,13 @@ def parse():
 
 
 def workload_config(args):
+    if args.workload == "short20k":
+        return {"workload": "batched psacak8: 20000 independent texts, lengths log-uniform 256 B..8 KiB, "
+                            "ACGT order-2 Markov (text i seeded by hash(seed, i)), one u32 SA per text "
+                            "(each sorted by one CTA in shared memory)",
+                "texts": 20000, "seed": args.seed, "engine": args.engine,
+                "l2_policy": "~46 MB of texts + ~183 MB of SAs (larger than L2 together); no flush",
+                "parallelism": "texts sharded across ranks (LPT)" if args.gpus > 1 else "single"}
     if args.workload == "batch4096":
         return {"workload": "batched psacak8: 4096 independent texts, lengths log-uniform 1 KiB..4 MiB, "
                             "ACGT order-2 Markov (text i seeded by hash(seed, i)), one u32 SA per text",
@@ -283,7 +291,7 @@ def run_serve(args):
 def run_b200(args):
     if args.workload == "serve":
         return run_serve(args)
-    if args.workload == "batch4096":
+    if args.workload in ("batch4096", "short20k"):
         return run_batch(args)
     if args.workload == "zipf32":
         return run_zipf32(args)
@@ -518,7 +526,8 @@ def _profile_roofline(ctx, build, torch, dev):
 
 
 def run_batch(args):
-    """Config 4: 4096 texts in one batched build, and the per-text loop beside it."""
+    """Config 4 (4096 texts of 1 KiB..4 MiB) or 20,000 short texts in one
+    batched build, and the per-text loop beside it."""
     import ctypes
     import torch
     import psacak_b200 as pk
@@ -530,7 +539,10 @@ def run_batch(args):
     dist = _dist_init(torch, world, local)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    texts = pb.batch_texts(count=4096, seed=args.seed)
+    if args.workload == "short20k":
+        texts = pb.batch_texts(count=20000, lo=256, hi=8 << 10, seed=args.seed)
+    else:
+        texts = pb.batch_texts(count=4096, seed=args.seed)
     lens = [t.size for t in texts]
     total_all = sum(lens)
     mine = pb.shard_lpt(lens, world)[rank]
@@ -539,6 +551,9 @@ def run_batch(args):
     n = int(buf.size)
     ctx = pk.Context(local)
     sched = {"engine": args.engine}
+    if args.workload == "short20k":
+        # texts below the default prefix-doubling cutoff: each sorted by one CTA in shared memory
+        sched["finish_below"] = 1 << 16
     d_texts = torch.from_numpy(buf).to(dev)
     d_sas = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)

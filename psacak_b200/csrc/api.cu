@@ -160,7 +160,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         if (names && bheads && ctx.sched.finish_below && n < ctx.sched.finish_below) {
             trace_push(ctx, level, width, n, 0, 0, 0);
             if (n <= SMALL_MAX && nbuckets <= 65535)  // in one CTA's shared memory
-                return small_sa<uint32_t>(ctx, names, SmallJobs{nullptr, nullptr, 1, n}, (uint32_t)nbuckets, sa, s);
+                return small_sa<uint32_t>(ctx, names, SmallJobs{nullptr, nullptr, 1, n, n}, (uint32_t)nbuckets, sa, s);
             return sort_by_doubling(ctx, names, bheads, nbuckets, n, sa, s);
         }
     } else {
@@ -168,7 +168,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
         if (ctx.sched.finish_below && n < ctx.sched.finish_below) {
             if (n <= SMALL_MAX) {  // in one CTA's shared memory
                 trace_push(ctx, level, width, n, 0, 0, 0);
-                return small_sa<uint8_t>(ctx, (const uint8_t *)text, SmallJobs{nullptr, nullptr, 1, n}, 256, sa, s);
+                return small_sa<uint8_t>(ctx, (const uint8_t *)text, SmallJobs{nullptr, nullptr, 1, n, n}, 256, sa, s);
             }
             DBuf<uint32_t> bnames, bh;
             PSK_TRY(bnames.init(ctx, n));

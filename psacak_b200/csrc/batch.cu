@@ -195,7 +195,9 @@ status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, ui
         PSK_TRY(d_ids.init(ctx, small.size()));
         PSK_CUDA(cudaMemcpyAsync(d_off.get(), h_off, ((size_t)ntexts + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
         PSK_CUDA(cudaMemcpyAsync(d_ids.get(), small.data(), small.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-        PSK_TRY(small_sa<uint8_t>(ctx, d_texts, SmallJobs{d_off.get(), d_ids.get(), (uint32_t)small.size(), 0}, 256,
+        uint64_t symbols = 0;
+        for (uint32_t i : small) symbols += h_off[i + 1] - h_off[i];
+        PSK_TRY(small_sa<uint8_t>(ctx, d_texts, SmallJobs{d_off.get(), d_ids.get(), (uint32_t)small.size(), 0, symbols}, 256,
                                   d_sas, s));
         // the host tables must outlive the copies
         PSK_CUDA(cudaStreamSynchronize(s));

@@ -220,7 +220,8 @@ status_t small_sa(Ctx &ctx, const C *text, SmallJobs jobs, uint32_t sigma, uint3
     uint32_t *queue = ctx.d_scalars + 40;
     PSK_CUDA(cudaMemsetAsync(queue, 0, sizeof(uint32_t), s));
     const uint32_t grid = jobs.count < (uint32_t)ctx.dev.num_sms ? jobs.count : (uint32_t)ctx.dev.num_sms;
-    PSK_PROF_LAUNCH(s, "small_strings", jobs.count, 0,
+    // algorithmic bytes: every string read once and its suffix array written once
+    PSK_PROF_LAUNCH(s, "small_strings", jobs.symbols, jobs.symbols * (sizeof(C) + sizeof(uint32_t)),
                     (k_small_sa<C><<<grid, SMALL_THREADS, SMALL_SMEM, s>>>(text, jobs, sigma, queue, sas, ctx.d_err)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;

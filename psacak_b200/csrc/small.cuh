@@ -20,6 +20,7 @@ struct SmallJobs {
     const uint32_t *ids;
     uint32_t count;
     uint64_t n;
+    uint64_t symbols;  // symbols of all strings together (host-side accounting only)
 };
 
 // Suffix arrays of the strings of `jobs` (each of at most SMALL_MAX
