@@ -27,9 +27,12 @@ def _worker(rank, world, port, lengths, q):
     mine = shard_lpt(lengths, world)[rank]
     got = [None] * world
     dist.all_gather_object(got, mine)
-    t = torch.tensor([10.0 * (rank + 1)], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    q.put((rank, got, float(t.item())))
+    # the reduction bench.py applies to every per-rank time
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    slowest = bench._max_over_ranks(torch, dist, torch.device("cpu"), 10.0 * (rank + 1))
+    q.put((rank, got, slowest))
     dist.barrier()
     dist.destroy_process_group()
 
