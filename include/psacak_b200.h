@@ -33,6 +33,7 @@ extern "C" {
 #define PSACAK_ECUDA (-3)     /* a CUDA runtime call failed */
 #define PSACAK_ETIMEOUT (-4)  /* a bounded device-side wait ran out */
 #define PSACAK_EINTERNAL (-5) /* a device-side consistency check failed */
+#define PSACAK_ECANCELED (-6) /* psacak_cancel ended the build */
 
 /* Induced-scan engine selection (psacak_schedule.engine). */
 #define PSACAK_ENGINE_AUTO 0     /* bucket scan for byte levels, doubling otherwise */
@@ -148,6 +149,18 @@ PSACAK_API int psacak8_batch(psacak_ctx *ctx, const uint8_t *const *texts, const
 PSACAK_API int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *offsets, uint32_t n_texts,
                                  uint32_t *d_sas, void *stream, const psacak_schedule *sched);
 
+/*
+ * psacak_cancel -- asks the build running on `ctx` to stop.  Safe to call
+ * from any thread while another thread is inside a call on `ctx`.  The build
+ * polls the request at its checkpoints (each recursion level, each round of
+ * the chain-doubling scans, each chunk or text of a batch), lets the work it
+ * has queued finish and returns PSACAK_ECANCELED; its output arrays are then
+ * unspecified and the context stays usable.  A request made while no build
+ * runs on `ctx` ends the next one at its first checkpoint.  The reference
+ * has no counterpart (its calls cannot be interrupted, src/lib.rs:64-82).
+ */
+PSACAK_API int psacak_cancel(psacak_ctx *ctx);
+
 /* Per-level records of the last build on `ctx` (see psacak_level_info). */
 PSACAK_API int psacak_get_trace(psacak_ctx *ctx, psacak_level_info *out, uint32_t cap, uint32_t *count);
 
@@ -222,6 +235,31 @@ PSACAK_API int psacak_lcp8_dev(psacak_ctx *ctx, const uint8_t *d_text, uint64_t 
                                uint32_t *d_lcp, void *stream);
 PSACAK_API int psacak_lcp32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, const uint32_t *d_sa,
                                 uint32_t *d_lcp, void *stream);
+
+/*
+ * FM-index of a byte text, over its BWT (psacak_bwt8_dev's output: n bytes
+ * and the primary index), on the device.  No counterpart in hucsmn/psacak;
+ * its suffix array (sentinel excluded, src/lib.rs:30-43) fixes the rows.
+ *
+ * psacak_fm_bytes: size of the index of an n-byte text (2 + 4/256 bytes per
+ *   text byte plus a 2 KiB header): the caller allocates it, 16-byte
+ *   aligned.
+ * psacak_fm_build_dev: fills d_fm (C array and rank checkpoints: a count of
+ *   every byte value per 2^16 positions and, relative to it, per 256).
+ * psacak_fm_count_dev: backward search of n_patterns patterns, pattern i
+ *   being bytes [d_offsets[i], d_offsets[i+1]) of d_patterns (d_offsets a
+ *   device array of n_patterns + 1 entries): d_ranges[2i], d_ranges[2i+1]
+ *   = the half-open range of suffix-array indices whose suffixes start with
+ *   the pattern (the occurrences are SA[lo .. hi), their number hi - lo; an
+ *   empty pattern matches [0, n)).  d_bwt is the BWT the index was built
+ *   from.
+ */
+PSACAK_API uint64_t psacak_fm_bytes(uint64_t n);
+PSACAK_API int psacak_fm_build_dev(psacak_ctx *ctx, const uint8_t *d_bwt, uint64_t n, uint64_t primary, void *d_fm,
+                                   void *stream);
+PSACAK_API int psacak_fm_count_dev(psacak_ctx *ctx, const void *d_fm, const uint8_t *d_bwt,
+                                   const uint8_t *d_patterns, const uint64_t *d_offsets, uint32_t n_patterns,
+                                   uint32_t *d_ranges, void *stream);
 
 /* Number of kernels the library launched since the context was created. */
 PSACAK_API uint64_t psacak_kernel_launches(psacak_ctx *ctx);

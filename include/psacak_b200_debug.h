@@ -39,6 +39,22 @@ PSACAK_API int psacak_debug_reduced8(psacak_ctx *ctx, const uint8_t *d_text, uin
                                      uint64_t cap, uint64_t *n_lms, uint64_t *k,
                                      const psacak_schedule *sched);
 
+/* Limits for the failure-path tests.  spin_limit: polls after which every
+ * bounded device wait of the calls on `ctx` gives up and the call returns
+ * PSACAK_ETIMEOUT (0 = the compiled limits, 2^22..2^24 polls; at most
+ * 2^31).  workspace_cap: most device workspace bytes a build on `ctx` may
+ * hold at once; a larger request fails with PSACAK_ENOMEM, as a failed
+ * allocation does (0 = no cap). */
+PSACAK_API int psacak_debug_set_limits(psacak_ctx *ctx, uint32_t spin_limit, uint64_t workspace_cap);
+
+/* Exclusive sum of n words of d_in into d_out by the single-pass look-back
+ * scan of every build, launched without its first tile: that tile's status
+ * words are never published, so the look-back of every other tile waits on
+ * a flag that nothing sets until its wait runs out.  Returns
+ * PSACAK_ETIMEOUT (after the bounded waits; keep the spin limit short) and
+ * leaves the context usable.  n must span at least two tiles (> 4096). */
+PSACAK_API int psacak_debug_stalled_scan(psacak_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint64_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,11 @@ void oracle_lcp8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint32_t *
 void oracle_lcp32(const uint32_t *text, uint64_t n, const uint32_t *sa, uint32_t *lcp);
 uint64_t oracle_bwt8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint8_t *bwt);
 
+/* Suffix-array indices [lo, hi) of the suffixes that start with pat[0, m),
+ * by binary search on the suffix array (checks the FM-index search). */
+void oracle_sa_range8(const uint8_t *text, uint64_t n, const uint32_t *sa, const uint8_t *pat, uint64_t m,
+                      uint64_t *lo, uint64_t *hi);
+
 /* saca_tiny (src/common.rs:13-25): naive comparison sort of the suffixes. */
 void oracle_saca_tiny8(const uint8_t *text, uint64_t n, uint32_t *sa);
 void oracle_saca_tiny32(const uint32_t *text, uint64_t n, uint32_t *sa);

@@ -34,6 +34,7 @@ PSACAK_ENOMEM = -2
 PSACAK_ECUDA = -3
 PSACAK_ETIMEOUT = -4
 PSACAK_EINTERNAL = -5
+PSACAK_ECANCELED = -6
 
 ENGINE_AUTO = 0
 ENGINE_BUCKET = 1
@@ -41,7 +42,7 @@ ENGINE_DOUBLING = 2
 
 _ERRNAMES = {
     PSACAK_EINVAL: "EINVAL", PSACAK_ENOMEM: "ENOMEM", PSACAK_ECUDA: "ECUDA",
-    PSACAK_ETIMEOUT: "ETIMEOUT", PSACAK_EINTERNAL: "EINTERNAL",
+    PSACAK_ETIMEOUT: "ETIMEOUT", PSACAK_EINTERNAL: "EINTERNAL", PSACAK_ECANCELED: "ECANCELED",
 }
 
 
@@ -120,6 +121,7 @@ def lib():
         L.psacak8_batch_dev.argtypes = [p, p, p, u32, p, p, p]
         L.psacak8_batch_dev.restype = i32
         L.psacak_get_trace.argtypes = [p, p, u32, ctypes.POINTER(u32)]
+        L.psacak_cancel.argtypes = [p]
         L.psacak_check_sa8_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
         L.psacak_check_sa32_dev.argtypes = [p, p, u64, p, ctypes.POINTER(i32), p]
         L.psacak_profile_enable.argtypes = [p, i32]
@@ -133,12 +135,17 @@ def lib():
         L.psacak_bwt8_dev.argtypes = [p, p, u64, p, p, ctypes.POINTER(u64), p]
         L.psacak_lcp8_dev.argtypes = [p, p, u64, p, p, p]
         L.psacak_lcp32_dev.argtypes = [p, p, u64, p, p, p]
-        for f in (L.psacak_isa_dev, L.psacak_bwt8_dev, L.psacak_lcp8_dev, L.psacak_lcp32_dev):
+        L.psacak_fm_bytes.argtypes = [u64]
+        L.psacak_fm_bytes.restype = u64
+        L.psacak_fm_build_dev.argtypes = [p, p, u64, u64, p, p]
+        L.psacak_fm_count_dev.argtypes = [p, p, p, p, p, u32, p, p]
+        for f in (L.psacak_isa_dev, L.psacak_bwt8_dev, L.psacak_lcp8_dev, L.psacak_lcp32_dev,
+                  L.psacak_fm_build_dev, L.psacak_fm_count_dev):
             f.restype = i32
         for name in ("psacak8", "psacak32", "psacak8_ctx", "psacak32_ctx", "psacak8_dev", "psacak32_dev",
                      "psacak8_batch", "psacak_get_trace", "psacak_check_sa8_dev", "psacak_check_sa32_dev",
                      "psacak_ctx_create", "psacak_ctx_destroy", "psacak_profile_enable", "psacak_profile_reset",
-                     "psacak_profile_get"):
+                     "psacak_profile_get", "psacak_cancel"):
             getattr(L, name).restype = i32
         _lib = L
         return L
@@ -259,6 +266,19 @@ class Context:
         _raise(lib().psacak_lcp32_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
                                       ctypes.c_void_p(d_lcp), ctypes.c_void_p(stream)))
 
+    def fm_build_dev(self, d_bwt, n, primary, d_fm, stream=0):
+        """FM-index of the BWT (divbwt convention) into d_fm, a device buffer
+        of fm_bytes(n) bytes."""
+        _raise(lib().psacak_fm_build_dev(self._h, ctypes.c_void_p(d_bwt), n, primary, ctypes.c_void_p(d_fm),
+                                         ctypes.c_void_p(stream)))
+
+    def fm_count_dev(self, d_fm, d_bwt, d_patterns, d_offsets, n_patterns, d_ranges, stream=0):
+        """Backward search: suffix-array ranges [lo, hi) of the patterns
+        (device pointers; offsets are n_patterns + 1 device uint64)."""
+        _raise(lib().psacak_fm_count_dev(self._h, ctypes.c_void_p(d_fm), ctypes.c_void_p(d_bwt),
+                                         ctypes.c_void_p(d_patterns), ctypes.c_void_p(d_offsets), n_patterns,
+                                         ctypes.c_void_p(d_ranges), ctypes.c_void_p(stream)))
+
     def check_sa8_dev(self, d_text, n, d_sa, stream=0):
         ok = ctypes.c_int(0)
         _raise(lib().psacak_check_sa8_dev(self._h, ctypes.c_void_p(d_text), n, ctypes.c_void_p(d_sa),
@@ -277,6 +297,12 @@ class Context:
         _raise(lib().psacak_get_trace(self._h, buf, 128, ctypes.byref(cnt)))
         return [dict(level=l.level, width=l.width, m=l.m, n_lms=l.n_lms, k=l.k, hash=l.hash)
                 for l in buf[:min(cnt.value, 128)]]
+
+    def cancel(self):
+        """Asks the build running on this context (or the next one) to stop;
+        that build raises PsacakError with code PSACAK_ECANCELED.  Safe to
+        call from another thread (psacak_cancel)."""
+        _raise(lib().psacak_cancel(self._h))
 
     def kernel_launches(self):
         return int(lib().psacak_kernel_launches(self._h))
@@ -304,6 +330,11 @@ def _sched_ptr(schedule):
             setattr(s, k, int(v))
         schedule = s
     return ctypes.byref(schedule)
+
+
+def fm_bytes(n):
+    """Bytes of the FM-index of an n-byte text (psacak_fm_bytes)."""
+    return int(lib().psacak_fm_bytes(n))
 
 
 NOALLOC_CHECK_MAX = 1 << 21
@@ -386,8 +417,11 @@ def _debug_lib():
         L.psacak_debug_exclusive_sum.argtypes = [p, p, p, u64]
         L.psacak_debug_types.argtypes = [p, p, u64, i32, p, p]
         L.psacak_debug_reduced8.argtypes = [p, p, u64, p, u64, ctypes.POINTER(u64), ctypes.POINTER(u64), p]
+        L.psacak_debug_set_limits.argtypes = [p, ctypes.c_uint32, u64]
+        L.psacak_debug_stalled_scan.argtypes = [p, p, p, u64]
         for name in ("psacak_debug_radix_sort_u64", "psacak_debug_radix_sort_u32", "psacak_debug_exclusive_sum",
-                     "psacak_debug_types", "psacak_debug_reduced8"):
+                     "psacak_debug_types", "psacak_debug_reduced8", "psacak_debug_set_limits",
+                     "psacak_debug_stalled_scan"):
             getattr(L, name).restype = i32
         L._debug_bound = True
     return L
@@ -411,6 +445,16 @@ class Stages:
 
     def types(self, d_text, n, width, d_types, d_lms):
         _raise(self.L.psacak_debug_types(self.ctx.handle, d_text, n, width, d_types, d_lms))
+
+    def set_limits(self, spin_limit=0, workspace_cap=0):
+        """Failure-path limits of the context: polls per bounded device wait
+        (0 = compiled limits) and most workspace bytes per build (0 = none)."""
+        _raise(self.L.psacak_debug_set_limits(self.ctx.handle, spin_limit, workspace_cap))
+
+    def stalled_scan(self, d_in, d_out, n):
+        """The look-back scan without its first tile: returns the status code
+        (PSACAK_ETIMEOUT once the waits run out) instead of raising."""
+        return int(self.L.psacak_debug_stalled_scan(self.ctx.handle, d_in, d_out, n))
 
     def reduced8(self, d_text, n, d_red, cap, schedule=None):
         n1 = ctypes.c_uint64(0)

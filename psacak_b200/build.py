@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "lib")
 OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(ROOT, "include")
 
-CU_SOURCES = ["prims.cu", "level.cu", "induce_doubling.cu", "induce_bucket.cu", "api.cu", "noalloc.cu", "batch.cu", "selector.cu", "gen.cu", "derived.cu", "hostio.cu", "small.cu"]
+CU_SOURCES = ["prims.cu", "level.cu", "induce_doubling.cu", "induce_bucket.cu", "api.cu", "noalloc.cu", "batch.cu", "selector.cu", "gen.cu", "derived.cu", "hostio.cu", "small.cu", "fmindex.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -149,6 +149,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
                      uint64_t n, uint32_t *sa, uint32_t level) {
     cudaStream_t s = ctx.stream;
     const uint32_t width = sizeof(C);
+    PSK_TRY(ctx.checkpoint());
     if (n <= 3) {
         PSK_TRY(tiny_sa(text, n, sa, s));
         trace_push(ctx, level, width, n, 0, 0, 0);
@@ -478,6 +479,7 @@ struct RankStore {
 status_t build_psacak32(Ctx &ctx, const uint32_t *text, uint64_t n, uint32_t *sa) {
     cudaStream_t s = ctx.stream;
     if (n == 0) return PSACAK_OK;
+    PSK_TRY(ctx.checkpoint());
     DBuf<uint32_t> k0, v0, k1, v1;
     PSK_TRY(k0.init(ctx, n));
     PSK_TRY(v0.init(ctx, n));
@@ -562,8 +564,9 @@ status_t ctx_init(Ctx &c, int device) {
     PSK_CUDA(cudaMalloc(&c.os.tickets, 64 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_hist, 256 * RADIX_MAX_CTAS * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_scalars, 64 * sizeof(uint32_t)));
-    PSK_CUDA(cudaMalloc(&c.d_err, sizeof(uint32_t)));
-    PSK_CUDA(cudaMemset(c.d_err, 0, sizeof(uint32_t)));
+    // error word + wait-limit override (common.cuh)
+    PSK_CUDA(cudaMalloc(&c.d_err, 2 * sizeof(uint32_t)));
+    PSK_CUDA(cudaMemset(c.d_err, 0, 2 * sizeof(uint32_t)));
     PSK_CUDA(cudaMalloc(&c.d_induced, 2 * sizeof(unsigned long long)));
     PSK_CUDA(cudaMemset(c.d_induced, 0, 2 * sizeof(unsigned long long)));
     c.scan_ctas = 4 * (uint32_t)c.dev.num_sms;
@@ -661,10 +664,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     status_t st;
     if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, nullptr, nullptr, 256, n, d_sa, 0);
     else st = build_psacak32(c, d_text, n, d_sa);
-    if (st != PSACAK_OK) {
-        cudaStreamSynchronize(c.stream);
-        return st;
-    }
+    if (st != PSACAK_OK) return c.fail(st);
     c.mark("final induce (level 0)", 0);
     PSK_TRY(c.sync());
     PSK_TRY(c.check_device_error());
@@ -872,6 +872,12 @@ int psacak32_dev(psacak_ctx *ctx, const uint32_t *d_text, uint64_t n, uint32_t *
     return run_dev<uint32_t>(ctx->c, d_text, n, d_sa, (cudaStream_t)stream, sched);
 }
 
+int psacak_cancel(psacak_ctx *ctx) {
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    ctx->c.cancel_req.store(1);
+    return PSACAK_OK;
+}
+
 int psacak_get_trace(psacak_ctx *ctx, psacak_level_info *out, uint32_t cap, uint32_t *count) {
     if (!ctx) return set_error(PSACAK_EINVAL, "null context");
     std::lock_guard<std::mutex> g(ctx->c.mu);
@@ -965,10 +971,7 @@ int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *o
     PSK_TRY(c.arena_prepare());
     ProfGuard pg(c);
     status_t st = build_batch(c, d_texts, offsets, n_texts, d_sas);
-    if (st != PSACAK_OK) {
-        cudaStreamSynchronize(c.stream);
-        return st;
-    }
+    if (st != PSACAK_OK) return c.fail(st);
     PSK_TRY(c.sync());
     PSK_TRY(c.check_device_error());
     PSK_TRY(profile_collect(c));
@@ -1111,6 +1114,48 @@ int psacak_debug_exclusive_sum(psacak_ctx *ctx, const uint32_t *d_in, uint32_t *
     PSK_TRY((c.scan<uint32_t, OpSum<uint32_t>>(CopyLoad{d_in}, CopyStore{d_out}, n, (uint32_t *)nullptr,
                                                OpSum<uint32_t>(), "scan")));
     return c.sync();
+}
+
+int psacak_debug_set_limits(psacak_ctx *ctx, uint32_t spin_limit, uint64_t workspace_cap) {
+    clear_error();
+    if (!ctx) return set_error(PSACAK_EINVAL, "null context");
+    if (spin_limit > 0x80000000u) return set_error(PSACAK_EINVAL, "spin limit %u above 2^31", spin_limit);
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.ws_cap = workspace_cap;
+    PSK_CUDA(cudaMemcpyAsync(c.d_err + 1, &spin_limit, sizeof(uint32_t), cudaMemcpyHostToDevice, c.own_stream));
+    PSK_CUDA(cudaStreamSynchronize(c.own_stream));
+    return PSACAK_OK;
+}
+
+int psacak_debug_stalled_scan(psacak_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint64_t n) {
+    clear_error();
+    if (!ctx || !d_in || !d_out) return set_error(PSACAK_EINVAL, "null argument");
+    constexpr uint64_t TILE = (uint64_t)LS_BLOCK * scan_ipt<uint32_t, CopyLoad>();
+    const uint64_t ntiles = ceil_div(n, TILE);
+    if (ntiles < 2 || ntiles > 0xFFFFFFFFull)
+        return set_error(PSACAK_EINVAL, "stalled scan: n = %llu must span 2 tiles of %llu", (unsigned long long)n,
+                         (unsigned long long)TILE);
+    std::lock_guard<std::mutex> g(ctx->c.mu);
+    Ctx &c = ctx->c;
+    PSK_CUDA(cudaSetDevice(c.dev.id));
+    c.stream = c.own_stream;
+    PSK_TRY(c.ensure_scan(n));
+    c.os.epoch = (c.os.epoch + 1) & ((1u << 30) - 1);
+    if (c.os.epoch == 0) c.os.epoch = 1;
+    uint32_t *ticket = c.os.tickets + (c.os.epoch & 63);
+    // the ticket starts at 1: tiles 1 .. ntiles-1 are claimed by the
+    // ntiles-1 CTAs (all in range), tile 0 by none
+    const uint32_t one = 1;
+    PSK_CUDA(cudaMemcpyAsync(ticket, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+    k_lbscan<uint32_t, OpSum<uint32_t>, CopyLoad, CopyStore><<<(uint32_t)(ntiles - 1), LS_BLOCK, 0, c.stream>>>(
+        CopyLoad{d_in}, CopyStore{d_out}, n, OpSum<uint32_t>(), c.ss.flags, ticket, c.os.epoch, (uint32_t)ntiles,
+        (uint32_t *)nullptr, c.d_err);
+    PSK_KCOUNT();
+    PSK_LAUNCH_CHECK();
+    PSK_TRY(c.sync());
+    return c.check_device_error();
 }
 
 int psacak_debug_types(psacak_ctx *ctx, const void *d_text, uint64_t n, int width, uint32_t *d_types,

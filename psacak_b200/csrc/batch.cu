@@ -178,6 +178,7 @@ status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, ui
     cudaStream_t s = ctx.stream;
     const uint64_t total = h_off[ntexts] - h_off[0];
     if (total == 0) return PSACAK_OK;
+    PSK_TRY(ctx.checkpoint());
     std::vector<uint32_t> small, big;
     for (uint32_t i = 0; i < ntexts; i++) {
         const uint64_t len = h_off[i + 1] - h_off[i];
@@ -223,6 +224,7 @@ status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, ui
     if (v == 256) {
         // all byte values in use: build every text on its own
         for (uint32_t i : big) {
+            PSK_TRY(ctx.checkpoint());
             uint64_t len = h_off[i + 1] - h_off[i];
             PSK_TRY(build_level<uint8_t>(ctx, d_texts + h_off[i], nullptr, nullptr, 256, len, d_sas + h_off[i], 0));
         }
@@ -230,6 +232,7 @@ status_t build_batch(Ctx &ctx, const uint8_t *d_texts, const uint64_t *h_off, ui
     }
     size_t t0 = 0;
     while (t0 < big.size()) {
+        PSK_TRY(ctx.checkpoint());
         size_t t1 = t0;
         uint64_t acc = 0;
         while (t1 < big.size()) {

@@ -54,6 +54,25 @@ __device__ __forceinline__ void dev_fail(uint32_t *err, uint32_t code) {
     if (err) atomicOr(err, code);
 }
 
+// The error word is err[0] of a two-word array; err[1], when non-zero,
+// replaces the compiled poll limit of every bounded wait (a test sets it
+// through psacak_debug_set_limits to make a wait run out quickly).
+// spin_spend keeps a wait's remaining budget in `left`: 0 means "not loaded
+// yet", so the override is read once, at the first poll that finds nothing
+// ready, and costs no register beyond the counter it replaces.  Returns true
+// when the budget is spent.
+__device__ __forceinline__ bool spin_spend(uint32_t &left, const uint32_t *err, uint32_t dflt) {
+    if (left == 0) {
+        uint32_t lim = dflt;
+        if (err) {
+            const uint32_t o = *(const volatile uint32_t *)(err + 1);
+            if (o) lim = o;
+        }
+        left = lim + 1;
+    }
+    return --left == 0;
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <time.h>
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -27,7 +28,7 @@ struct Ctx {
     uint32_t *m_pinned = nullptr;   // its device view
     uint32_t *d_hist = nullptr;     // 256 * RADIX_MAX_CTAS radix histograms
     uint32_t *d_scalars = nullptr;  // 64 device scalars
-    uint32_t *d_err = nullptr;      // device error word
+    uint32_t *d_err = nullptr;      // device error word, then the wait-limit override (common.cuh)
     uint32_t *h_hist = nullptr;     // pinned, mapped copy of the radix digit counts
     uint32_t *m_hist = nullptr;     // its device view
     OnesweepScratch os;             // look-back status words of the onesweep kernels
@@ -46,6 +47,20 @@ struct Ctx {
     Profiler prof;
     unsigned long long *d_induced = nullptr;  // entries scattered by the bucket scans
     std::mutex mu;
+    // Most workspace bytes a build may hold at once (0 = no cap); a larger
+    // request fails with PSACAK_ENOMEM as a failed allocation would.
+    uint64_t ws_cap = 0;
+    // Set by psacak_cancel from any thread; the build polls it at its
+    // checkpoints (recursion levels, doubling rounds, batch chunks).
+    std::atomic<uint32_t> cancel_req{0};
+    // Checkpoint of a build: consumes a pending cancellation request, lets
+    // the work already queued finish (so no buffer is recycled under a
+    // running kernel) and ends the build with PSACAK_ECANCELED.
+    status_t checkpoint() {
+        if (!cancel_req.load(std::memory_order_relaxed) || !cancel_req.exchange(0)) return PSACAK_OK;
+        cudaStreamSynchronize(stream);
+        return set_error(PSACAK_ECANCELED, "the build was cancelled");
+    }
 
     // Host destination of the final suffix array, set by host-pointer calls
     // whose output buffer is pinned: the level-0 bucket scans send each
@@ -107,6 +122,11 @@ struct Ctx {
         size_t bytes = count * sizeof(T);
         if (bytes == 0) bytes = 16;
         bytes = (bytes + 255) & ~(size_t)255;
+        if (ws_cap && arena_vtop + bytes > ws_cap) {
+            *p = nullptr;
+            return set_error(PSACAK_ENOMEM, "device allocation of %zu bytes failed: workspace cap of %llu bytes",
+                             bytes, (unsigned long long)ws_cap);
+        }
         arena_vtop += bytes;
         if (arena_vtop > arena_high) arena_high = arena_vtop;
         if (arena && arena_top + bytes <= arena_size) {
@@ -231,6 +251,22 @@ struct Ctx {
             return set_error(PSACAK_EINTERNAL, "device-side consistency check failed (0x%x)", e);
         }
         return PSACAK_OK;
+    }
+    // Ends a failed call: waits for the work already queued, then reports a
+    // device-side timeout in preference to the host-side symptom it caused
+    // (a count that did not add up), and clears the error word so that the
+    // next call starts clean.  Cancellation and argument errors pass through.
+    status_t fail(status_t st) {
+        cudaStreamSynchronize(stream);
+        if (st == PSACAK_ECANCELED || st == PSACAK_EINVAL) return st;
+        uint32_t e = 0;
+        if (read_u32(d_err, &e) != PSACAK_OK) return st;
+        if (e) {
+            cudaMemsetAsync(d_err, 0, sizeof(uint32_t), stream);
+            cudaStreamSynchronize(stream);
+            if (e & DEVERR_TIMEOUT) return set_error(PSACAK_ETIMEOUT, "a bounded device wait ran out (0x%x)", e);
+        }
+        return st;
     }
 };
 

@@ -38,10 +38,21 @@ __global__ void k_phi(const uint32_t *__restrict__ sa, uint64_t n, uint32_t *phi
     }
 }
 
+// Symbols one thread compares for an irreducible position before handing
+// it to a whole CTA (k_plcp_long): a long run of one character has a single
+// irreducible position whose PLCP is about the run's length, which one
+// thread would walk alone.
+constexpr uint32_t LCP_THREAD_MAX = 1024;
+constexpr int LCP_LONG_BLOCK = 256;
+constexpr int LCP_LONG_SYMS = 16;  // per thread and step: 4096 symbols per CTA step
+
 // PLCP of the irreducible positions (by comparison) and their bitmap.
+// Comparisons that reach LCP_THREAD_MAX symbols are listed in `longs` (up to
+// `long_cap`; beyond it the thread goes on alone) with their PLCP so far.
 template <class C>
 __global__ void k_plcp_irreducible(const C *__restrict__ text, uint64_t n, const uint32_t *__restrict__ phi,
-                                   uint32_t *plcp, uint32_t *irr) {
+                                   uint32_t *plcp, uint32_t *irr, uint32_t *longs, uint32_t *nlong,
+                                   uint32_t long_cap) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32
     for (uint64_t jb = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); jb < n; jb += stride) {
@@ -52,13 +63,65 @@ __global__ void k_plcp_irreducible(const C *__restrict__ text, uint64_t n, const
             ir = j == 0 || p == PHI_NONE || p == 0 || text[j - 1] != text[p - 1];
             if (ir) {
                 uint64_t h = 0;
-                if (p != PHI_NONE)
-                    while (j + h < n && p + h < n && text[j + h] == text[p + h]) h++;
+                if (p != PHI_NONE) {
+                    while (h < LCP_THREAD_MAX && j + h < n && p + h < n && text[j + h] == text[p + h]) h++;
+                    if (h == LCP_THREAD_MAX && j + h < n && p + h < n) {
+                        const uint32_t slot = atomicAdd(nlong, 1u);
+                        if (slot < long_cap) longs[slot] = (uint32_t)j;
+                        else
+                            while (j + h < n && p + h < n && text[j + h] == text[p + h]) h++;
+                    }
+                }
                 plcp[j] = (uint32_t)h;
             }
         }
         const uint32_t word = __ballot_sync(FULL_MASK, ir);
         if (lane == 0 && jb < n) irr[jb >> 5] = word;
+    }
+}
+
+// The listed long comparisons, one CTA each: every step compares the next
+// LCP_LONG_BLOCK x LCP_LONG_SYMS symbols of both suffixes, each thread a
+// stretch of LCP_LONG_SYMS, and the CTA takes the first mismatch.
+template <class C>
+__global__ void __launch_bounds__(LCP_LONG_BLOCK) k_plcp_long(const C *__restrict__ text, uint64_t n,
+                                                             const uint32_t *__restrict__ phi, uint32_t *plcp,
+                                                             const uint32_t *__restrict__ longs,
+                                                             const uint32_t *nlong, uint32_t long_cap) {
+    __shared__ uint32_t s_min[LCP_LONG_BLOCK / 32];
+    const uint32_t count = *nlong < long_cap ? *nlong : long_cap;
+    constexpr uint32_t STEP = LCP_LONG_BLOCK * LCP_LONG_SYMS;
+    for (uint32_t it = blockIdx.x; it < count; it += gridDim.x) {
+        const uint64_t j = longs[it];
+        const uint64_t p = phi[j];
+        uint64_t h = plcp[j];
+        const uint64_t lim = n - (j > p ? j : p);  // both suffixes end at n
+        while (true) {
+            uint32_t first = 0xFFFFFFFFu;  // this thread's first mismatch in the step
+            const uint64_t o = h + (uint64_t)threadIdx.x * LCP_LONG_SYMS;
+            for (uint32_t k = 0; k < LCP_LONG_SYMS; k++) {
+                const uint64_t q = o + k;
+                if (q >= lim || text[j + q] != text[p + q]) {
+                    first = (uint32_t)(q - h);
+                    break;
+                }
+            }
+            for (int d = 16; d > 0; d >>= 1) {
+                const uint32_t other = __shfl_xor_sync(FULL_MASK, first, d);
+                first = other < first ? other : first;
+            }
+            if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = first;
+            __syncthreads();
+            uint32_t m = 0xFFFFFFFFu;
+            for (int w = 0; w < LCP_LONG_BLOCK / 32; w++) m = s_min[w] < m ? s_min[w] : m;
+            __syncthreads();
+            if (m != 0xFFFFFFFFu) {
+                h += m;
+                break;
+            }
+            h += STEP;
+        }
+        if (threadIdx.x == 0) plcp[j] = (uint32_t)h;
     }
 }
 
@@ -145,13 +208,21 @@ static int lcp_dev(psacak_ctx *ctx, const C *d_text, uint64_t n, const uint32_t 
     c.stream = stream ? (cudaStream_t)stream : c.own_stream;
     if (n == 0) return PSACAK_OK;
     cudaStream_t s = c.stream;
-    DBuf<uint32_t> plcp, irr;
+    DBuf<uint32_t> plcp, irr, longs;
     PSK_TRY(plcp.init(c, n));
     PSK_TRY(irr.init(c, ceil_div(n, 32) + 1));
+    const uint32_t long_cap = (uint32_t)(n / 64 + 1024);
+    PSK_TRY(longs.init(c, long_cap));
+    uint32_t *nlong = c.d_scalars + 42;
+    PSK_CUDA(cudaMemsetAsync(nlong, 0, sizeof(uint32_t), s));
     uint32_t *phi = d_lcp;  // the output holds phi until the final gather
     PSK_PROF_LAUNCH(s, "lcp_phi", n, 12ull * n, (k_phi<<<grid_for_n(n), 256, 0, s>>>(d_sa, n, phi, c.d_err)));
     PSK_PROF_LAUNCH(s, "lcp_irreducible", n, 0,
-                    (k_plcp_irreducible<C><<<grid_for_n(n), 256, 0, s>>>(d_text, n, phi, plcp, irr)));
+                    (k_plcp_irreducible<C><<<grid_for_n(n), 256, 0, s>>>(d_text, n, phi, plcp, irr, longs, nlong,
+                                                                          long_cap)));
+    PSK_PROF_LAUNCH(s, "lcp_long", n, 0,
+                    (k_plcp_long<C><<<2 * (uint32_t)c.dev.num_sms, LCP_LONG_BLOCK, 0, s>>>(d_text, n, phi, plcp, longs,
+                                                                                           nlong, long_cap)));
     PSK_TRY((c.scan<uint32_t, OpMax<uint32_t>>(AnchorLoad{irr}, AnchorStore{plcp, c.d_err}, n, (uint32_t *)nullptr,
                                                OpMax<uint32_t>(), "lcp_reducible")));
     PSK_PROF_LAUNCH(s, "lcp_gather", n, 12ull * n, (k_lcp_gather<<<grid_for_n(n), 256, 0, s>>>(d_sa, n, plcp, d_lcp)));

@@ -368,6 +368,7 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
     if (Wg != (uint32_t *)k1 || Wv != Wg + n)
         return set_error(PSACAK_EINTERNAL, "doubling rounds: work list outside its radix pair");
     for (uint64_t h = 1; cnt > 0; h <<= 1) {
+        PSK_TRY(ctx.checkpoint());
         const int GB = bitlen(ngroups > 0 ? ngroups - 1 : 0);
         if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
         uint64_t gblocks = ceil_div(cnt, 256 * 16);

@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t
         } else {
             if (lane == 0) os_store(flags + (uint64_t)tile * NF + f, os_word(epoch, OS_FLAG_AGG, tot_f));
             int64_t top = (int64_t)tile - 1;  // nearest tile not yet accounted for
-            uint32_t spins = 0;
+            uint32_t left = 0;  // poll budget (spin_spend)
             while (true) {
                 const int64_t t = top - (int64_t)lane;
                 bool ready = true;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t
                 const int last = pmask ? __ffs(pmask) - 1 : 31;  // lanes 0..last are needed
                 const uint32_t need = last == 31 ? FULL_MASK : ((1u << (last + 1)) - 1u);
                 if (nready & need) {
-                    if (++spins > LS_SPIN_LIMIT) {
+                    if (spin_spend(left, err, LS_SPIN_LIMIT)) {
                         dev_fail(err, DEVERR_TIMEOUT);
                         break;
                     }

@@ -74,7 +74,7 @@ __device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile,
     os_store(my, os_word(epoch, OS_FLAG_AGG, count));
     uint32_t excl = 0;
     int64_t t = (int64_t)tile - 1;
-    uint32_t spins = 0;
+    uint32_t left = 0;  // poll budget (spin_spend)
     while (t >= 0) {
         // WINDOW predecessors per step, their loads in flight together (a
         // walk over tiles that have only published their counts costs one
@@ -96,7 +96,7 @@ __device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile,
             }
         }
         if (found) break;
-        if (k == 0 && ++spins > OS_SPIN_LIMIT) {
+        if (k == 0 && spin_spend(left, err, OS_SPIN_LIMIT)) {
             dev_fail(err, DEVERR_TIMEOUT);
             break;
         }

@@ -101,10 +101,9 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
             bulk_g2s(s_k, kin + base, TILE * (uint32_t)sizeof(K), &s_bar);
             bulk_g2s(s_v, vin + base, TILE * (uint32_t)sizeof(V), &s_bar);
         }
-        if (!mbar_wait_bounded(&s_bar, 0, err)) {
-            mbar_wait_bounded(&s_bar, 0, err);  // let the copies land before the CTA retires
-            return;
-        }
+        // one outcome for the whole CTA: the ranking below uses
+        // __syncthreads and full-warp ballots
+        if (!mbar_wait_cta(&s_bar, 0, err)) return;
     } else {
         for (uint32_t i = threadIdx.x; i < cnt; i += OS_BLOCK) {
             s_k[i] = kin[base + i];

@@ -4,9 +4,9 @@
 // One elected thread arms the barrier with the expected byte count and
 // issues the copies; every thread then waits on the barrier's phase.  No
 // cluster multicast is used: each CTA copies into its own shared memory.
-// Waits are bounded; a wait that gives up reports DEVERR_TIMEOUT and the
-// caller waits once more (bounded) before it lets the CTA retire, so no
-// copy is left writing into shared memory that has been released.
+// Waits are bounded; a wait that gives up reports DEVERR_TIMEOUT, and the
+// CTA agrees on the outcome and waits once more (bounded) before it retires,
+// so no copy is left writing into shared memory that has been released.
 #pragma once
 
 #include "common.cuh"
@@ -50,11 +50,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 
 // Bounded wait for the given phase; false (and DEVERR_TIMEOUT) if it did not
 // complete within TMA_SPIN_LIMIT polls.
+// The outcome is this thread's own: a caller whose threads go on to
+// block-wide barriers or full-warp votes must agree on it first (see
+// mbar_wait_cta).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t *err) {
-    for (uint32_t spins = 0; spins < TMA_SPIN_LIMIT; spins++)
+    uint32_t left = 0;
+    while (true) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (spin_spend(left, err, TMA_SPIN_LIMIT)) break;
+    }
     dev_fail(err, DEVERR_TIMEOUT);
     return false;
+}
+
+// Bounded wait by every thread of the CTA with one CTA-wide outcome: if any
+// thread's wait ran out, every thread waits once more (bounded; the copies
+// may still be landing in shared memory) and all of them get false, so the
+// CTA retires as a whole instead of leaving some threads in later barriers.
+// Must be called by all threads of the CTA.
+__device__ __forceinline__ bool mbar_wait_cta(uint64_t *bar, uint32_t parity, uint32_t *err) {
+    const bool ok = mbar_wait_bounded(bar, parity, err);
+    if (__syncthreads_or(!ok)) {
+        mbar_wait_bounded(bar, parity, err);
+        return false;
+    }
+    return true;
 }
 
 }  // namespace psk

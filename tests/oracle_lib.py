@@ -41,6 +41,7 @@ def lib():
         _lib.oracle_lcp32.argtypes = [p, u64, p, p]
         _lib.oracle_bwt8.argtypes = [p, u64, p, p]
         _lib.oracle_bwt8.restype = u64
+        _lib.oracle_sa_range8.argtypes = [p, u64, p, p, u64, p, p]
         _lib.oracle_saca_tiny8.argtypes = [p, u64, p]
         _lib.oracle_saca_tiny32.argtypes = [p, u64, p]
         _lib.oracle_translate_sample.argtypes = [p, u64, p]
@@ -162,3 +163,14 @@ def reduced8(text):
     k = ctypes.c_uint64(0)
     n1 = lib().oracle_reduced8(_ptr(t), t.size, _ptr(out), out.size, ctypes.byref(k))
     return out[:n1].copy(), int(k.value)
+
+
+def sa_range8(text, sa, pattern):
+    """[lo, hi) of suffix-array indices whose suffixes start with `pattern`."""
+    t = np.ascontiguousarray(text, dtype=np.uint8)
+    s = np.ascontiguousarray(sa, dtype=np.uint32)
+    pt = np.frombuffer(bytes(pattern), np.uint8).copy() if not isinstance(pattern, np.ndarray) else \
+        np.ascontiguousarray(pattern, dtype=np.uint8)
+    lo, hi = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    lib().oracle_sa_range8(_ptr(t), t.size, _ptr(s), _ptr(pt), pt.size, ctypes.byref(lo), ctypes.byref(hi))
+    return int(lo.value), int(hi.value)

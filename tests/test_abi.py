@@ -71,3 +71,11 @@ def test_init_rejects_bad_devices_and_shutdown_without_context():
     lib = pk.lib()
     assert lib.psacak_init(-1) == pk.PSACAK_EINVAL
     assert lib.psacak_shutdown() == 0
+
+
+def test_failure_path_entry_points_reject_null_context():
+    lib = pk.lib()
+    assert lib.psacak_cancel(None) == pk.PSACAK_EINVAL
+    dl = pk._debug_lib()
+    assert dl.psacak_debug_set_limits(None, 0, 0) == pk.PSACAK_EINVAL
+    assert dl.psacak_debug_stalled_scan(None, None, None, 0) == pk.PSACAK_EINVAL

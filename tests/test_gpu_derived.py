@@ -61,3 +61,29 @@ def test_lcp_u32(ctx):
         lcp = torch.empty(n, dtype=torch.int32, device="cuda")
         ctx.lcp32_dev(dt.data_ptr(), n, ds.data_ptr(), lcp.data_ptr())
         assert (lcp.cpu().numpy().view(np.uint32) == o.lcp(t, sa)).all()
+
+
+def test_lcp_run_heavy_texts_finish_quickly(ctx):
+    """Long runs of one character: the single irreducible position of a run
+    has a PLCP about the run's length, compared by a whole CTA rather than
+    one thread; mixed with periodic stretches whose irreducible positions
+    cross the per-thread limit by various amounts."""
+    import time
+    rng = np.random.default_rng(8)
+    texts = [np.concatenate([np.full(8 << 20, 65, np.uint8), rng.integers(65, 69, 1000).astype(np.uint8)]),
+             np.concatenate([rng.integers(65, 69, 5000).astype(np.uint8), np.full(3_000_017, 67, np.uint8),
+                             np.tile(np.frombuffer(b"ACGTTGCA", np.uint8), 200_000),
+                             np.full(1023, 71, np.uint8), np.full(1025, 84, np.uint8)]),
+             np.tile(synth.iid(5000, b"ACGT", seed=3), 300)]
+    for t in texts:
+        n = t.size
+        sa = o.psacak8(t)
+        dt = torch.from_numpy(t.copy()).cuda()
+        ds = torch.from_numpy(sa.view(np.int32).copy()).cuda()
+        lcp = torch.empty(n, dtype=torch.int32, device="cuda")
+        ctx.lcp8_dev(dt.data_ptr(), n, ds.data_ptr(), lcp.data_ptr())  # warm-up
+        t0 = time.perf_counter()
+        ctx.lcp8_dev(dt.data_ptr(), n, ds.data_ptr(), lcp.data_ptr())
+        secs = time.perf_counter() - t0
+        assert (lcp.cpu().numpy().view(np.uint32) == o.lcp(t, sa)).all(), n
+        assert secs < 0.5, (n, secs)

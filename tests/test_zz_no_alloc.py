@@ -49,6 +49,26 @@ def test_noalloc_check_matches_allocating_check(n):
             assert not ctx.check_sa8_dev(dt.data_ptr(), n, bad.data_ptr(), stream.cuda_stream)
 
 
+def test_noalloc_check_allocates_no_device_memory():
+    n = pk.NOALLOC_CHECK_MAX
+    text = synth.genome(n, seed=32)
+    stream = torch.cuda.current_stream()
+    with pk.Context(0) as ctx:
+        dt = torch.from_numpy(text).cuda()
+        ds = torch.empty(n, dtype=torch.int32, device="cuda")
+        ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        # the first call loads the library's module and looks up the array
+        assert _noalloc(dt.data_ptr(), n, ds.data_ptr(), stream.cuda_stream) == (pk.PSACAK_OK, 1)
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        for _ in range(4):
+            assert _noalloc(dt.data_ptr(), n, ds.data_ptr(), stream.cuda_stream) == (pk.PSACAK_OK, 1)
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0
+
+
 def test_noalloc_check_rejects_oversize():
     n = pk.NOALLOC_CHECK_MAX + 1
     dt = torch.zeros(n, dtype=torch.uint8, device="cuda")
