@@ -55,9 +55,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
-    ap.add_argument("--cpu-window", type=int, default=16 << 20, help="bytes per 1-core CPU-oracle sample")
     ap.add_argument("--cpu-sample", type=int, default=64 << 20,
-                    help="bytes per all-core CPU sample (reference arm, all-core baseline)")
+                    help="bytes of the CPU samples (reference arm, 1-core and all-core baselines)")
     ap.add_argument("--engine", type=int, default=0, help="psacak_schedule.engine (0 = auto)")
     ap.add_argument("--profile-json", default="", help="also write per-kernel stats here")
     ap.add_argument("--workload", default="genome1g",
@@ -67,9 +66,17 @@ def parse():
                          "short20k (20,000 texts of 256 B..8 KiB in one batched build)")
     ap.add_argument("--requests", type=int, default=20000, help="serve: number of requests")
     ap.add_argument("--load", type=float, default=0.7, help="serve: arrival rate / measured capacity")
+    ap.add_argument("--workers", type=int, default=2, help="serve: worker threads (one context each)")
     ap.add_argument("--regret-sample", type=int, default=200, help="serve: requests whose selector choice is checked against exhaustive autotune")
     ap.add_argument("--plain-texts", type=int, default=0,
                     help="batch4096: time the per-text loop on this many texts (0 = all)")
+    ap.add_argument("--no-tune", action="store_true", help="batched forms: skip the autotuner (library default)")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="genome1g: skip the batched form (4096 texts) that the default run reports beside it")
+    ap.add_argument("--batch-steps", type=int, default=3,
+                    help="genome1g: timed steps of the batched form (each ~0.7 s)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="genome1g: skip the exhaustive-autotune form of the headline text")
     ap.add_argument("--single-build", action="store_true",
                     help="build the workload once and exit (for ncu launch lists)")
     return ap.parse_args()
@@ -202,9 +209,10 @@ def cpu_baseline_all(text, window):
     oracle_lib.psacak8_par(w, cores)
     dt = time.perf_counter() - t0
     return {"value": window / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "first %d bytes of the workload text, one build with the reference's pipelined induced scans "
-                      "(fetch / induce / flush over 128Ki blocks) on %d threads; C++ restatement, the Rust crate is "
-                      "unbuildable here; naming and the inner levels run serially" % (window, cores),
+            "sample": "first %d bytes of the workload text, one build on %d threads: the reference's pipelined "
+                      "induced scans (fetch / induce / flush over 128Ki blocks), its chunked parallel naming, "
+                      "prefetching u32 scans on the inner levels; C++ restatement, the Rust crate is unbuildable "
+                      "here" % (window, cores),
             "seconds": dt}
 
 
@@ -235,6 +243,7 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     sample = min(args.cpu_sample, args.bytes)
     text = synth.genome(sample, seed=args.seed)  # the workload text's first `sample` bytes
+    one = cpu_baseline_single(text, sample)  # the serial restatement on the same sample, one core
     times = []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -250,10 +259,12 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
         "config": workload_config(args),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "per step, one build of the first %d bytes of the workload text with the "
-                                   "reference's pipelined induced scans (fetch / induce / flush, 128Ki blocks) on "
-                                   "%d threads; C++ restatement of the reference (the Rust crate is unbuildable on "
-                                   "this image); naming and inner levels serial" % (sample, cores)},
+                         "sample": "per step, one build of the first %d bytes of the workload text on %d threads: "
+                                   "the reference's pipelined induced scans (fetch / induce / flush, 128Ki blocks), "
+                                   "its chunked parallel naming, prefetching u32 scans on the inner levels; C++ "
+                                   "restatement of the reference (the Rust crate is unbuildable on this image)"
+                                   % (sample, cores)},
+        "cpu_baseline_one_core": one,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -262,7 +273,8 @@ def run_reference(args):
 
 # -- GPU arm -------------------------------------------------------------------
 def run_serve(args):
-    """Config 5: Poisson stream of build requests with the learned selector."""
+    """Config 5: Poisson stream of build requests served from host buffers by
+    two worker threads, with the learned schedule selector."""
     import torch
     import psacak_b200 as pk
     from psacak_b200 import selector as sel
@@ -273,16 +285,40 @@ def run_serve(args):
     ctx = pk.Context(0)
     model = os.path.join(ROOT, "psacak_b200", "models", "selector.npz")
     net = sel.Selector.load(ctx, model) if os.path.exists(model) else None
-    res = serve.run(ctx, net, count=args.requests, seed=args.seed, load=args.load,
-                    autotune_sample=args.regret_sample, log=lambda m: print(m, file=sys.stderr, flush=True))
+    best_fixed = None
+    rep = os.path.join(ROOT, "psacak_b200", "models", "selector_report.json")
+    if os.path.exists(rep):
+        with open(rep) as f:
+            best_fixed = json.load(f).get("best_fixed_index")
+
+    def check(i, text, sa):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        want = oracle_lib.psacak8(text) if text.dtype == np.uint8 else oracle_lib.psacak32(text)
+        return bool(np.array_equal(sa, want))
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    res = serve.run(net, count=args.requests, seed=args.seed, load=args.load, workers=args.workers,
+                    autotune_sample=args.regret_sample, best_fixed=best_fixed,
+                    log=lambda m: print(m, file=sys.stderr, flush=True),
+                    check=None if args.no_verify else check)
+    clk = clocks.stop()
     line = {"metric": "serving throughput (suffixes/s) with p50/p99 latency, learned schedule selector",
             "value": res["throughput_suffixes_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32", "data": "synthetic",
-            "config": {"workload": "%d requests, Poisson arrivals at %.0f%% of measured capacity, lengths log-uniform "
-                                   "4 KiB..64 MiB symbols, half u8 ACGT / half u32 over 2^16 (device-generated "
-                                   "i.i.d.)" % (args.requests, 100 * args.load), "seed": args.seed,
-                       "selector": "trained model" if net is not None else "none (default schedule)"},
-            "serving": res}
+            "config": {"workload": "%d requests, Poisson arrivals at %.0f%% of the capacity measured with the same "
+                                   "%d workers busy, lengths log-uniform 4 KiB..64 MiB symbols, a quarter each of "
+                                   "u8 ACGT i.i.d., u8 ACGT genome-like, u32 over 2^16 i.i.d., u32 over 2^16 Zipf "
+                                   "with repeats; texts in pageable host memory, suffix arrays back to pinned host "
+                                   "buffers, copies inside the latency" % (args.requests, 100 * args.load,
+                                                                          args.workers),
+                       "seed": args.seed,
+                       "selector": "trained model" if net is not None else "none (library default schedule)"},
+            "e2e": {"value": res["throughput_suffixes_per_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "every request's text upload and SA download are inside its latency"},
+            "clocks": clk, "serving": res}
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -408,9 +444,11 @@ def run_b200(args):
     # statistics (inference kernel), timed the same way as the plain form
     learned = None
     model = os.path.join(ROOT, "psacak_b200", "models", "selector.npz")
+    net = None
     if os.path.exists(model) and not args.single_build:
         from psacak_b200 import selector as sel
         net = sel.Selector.load(ctx, model)
+    if net is not None:
         feats = sel.features(ctx, d_text.data_ptr(), n, 1)
         choice, _ = net.predict(feats)
         lsched = dict(sel.SCHEDULES[choice])
@@ -426,6 +464,34 @@ def run_b200(args):
         lok = None if args.no_verify else ctx.check_sa8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream)
         learned = {"value": world * n / (lms_ / 1000.0), "unit": UNIT, "ms_per_step": lms_, "schedule": lsched,
                    "verified": lok, "hbm_gbs_algorithmic_build": build_bytes / (lms_ / 1000.0) / 1e9}
+    # autotuned form: exhaustive search over the selector's schedules on
+    # this text (the selector's fallback and yardstick), timed as above
+    autotuned = None
+    if not args.no_autotune and not args.single_build:
+        from psacak_b200 import autotune, selector as sel
+        t0 = time.perf_counter()
+        tf = autotune.device_timer(
+            lambda sc: ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, sc))
+        best_i, table = autotune.exhaustive(tf, sel.SCHEDULES)
+        tune_s = time.perf_counter() - t0
+        asched = dict(sel.SCHEDULES[best_i])
+        for _ in range(max(1, args.warmup)):
+            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, asched)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, asched)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ams = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+        aok = None if args.no_verify else ctx.check_sa8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream)
+        autotuned = {"value": world * n / (ams / 1000.0), "unit": UNIT, "ms_per_step": ams, "schedule": asched,
+                     "verified": aok, "search": "exhaustive over %d schedules (min of 1 build each, after a "
+                                                "warm-up build)" % len(sel.SCHEDULES),
+                     "search_seconds": tune_s, "search_ms": table,
+                     "hbm_gbs_algorithmic_build": build_bytes / (ams / 1000.0) / 1e9}
+        if learned is not None:
+            learned["regret_vs_autotuned"] = learned["ms_per_step"] / ams - 1.0
     if args.profile_json and rank == 0:
         with open(args.profile_json, "w") as f:
             json.dump({"stats": stats, "trace": trace, "ms_per_step": ms}, f, indent=1)
@@ -463,9 +529,28 @@ def run_b200(args):
             # scans) must equal the checked device-resident array
             e2e["verified"] = bool(verified) and bool(np.array_equal(hs, d_sa.cpu().numpy().view(np.uint32)))
 
+    # batched form (4096 texts of 1 KiB..4 MiB, about 2 GiB) on the same GPU:
+    # autotuned chunk size / block shape, beside the per-text loop
+    batched = None
+    if args.workload == "genome1g" and not args.no_batch and not args.single_build:
+        from psacak_b200 import batch as pb
+        del d_text, d_sa
+        torch.cuda.empty_cache()
+        btexts = pb.batch_texts(count=4096, seed=args.seed)
+        batched = measure_batch(args, torch, ctx, dev, dist, world, rank, btexts, args.batch_steps,
+                                max(3, args.warmup), tune=not args.no_tune, e2e_steps=args.e2e_steps,
+                                cpu=False)
+        batched["config"] = {"workload": "batched psacak8: 4096 independent texts, lengths log-uniform "
+                                         "1 KiB..4 MiB, ACGT order-2 Markov (text i seeded by hash(seed, i)), "
+                                         "one u32 SA per text", "texts": 4096, "seed": args.seed,
+                             "l2_policy": "inputs larger than L2 (~2 GiB of texts, ~8 GiB of SAs); no flush",
+                             "parallelism": "texts sharded across ranks (LPT)" if world > 1 else "single"}
+        batched["scaling"] = "strong"
+
     cpu = cpu_all = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline_single(text, min(args.cpu_window, n))
+        # both on the same prefix, so that the two rates compare
+        cpu = cpu_baseline_single(text, min(args.cpu_sample, n))
         cpu_all = cpu_baseline_all(text, min(args.cpu_sample, n))
 
     if rank == 0:
@@ -473,7 +558,8 @@ def run_b200(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": workload_config(args),
-            "e2e": e2e, "roofline": roofline, "learned_schedule": learned,
+            "e2e": e2e, "roofline": roofline, "learned_schedule": learned, "autotuned_schedule": autotuned,
+            "batched": batched,
             "plain_schedule": {"engine": args.engine, "note": "library default schedule (the value above)"},
             "hbm_gbs_algorithmic_build": build_gbs,
             "build_algorithmic_bytes": build_bytes,
@@ -525,43 +611,52 @@ def _profile_roofline(ctx, build, torch, dev):
             "share_of_profiled_time": dom["ms"] / total_ms if total_ms else None}, stats
 
 
-def run_batch(args):
-    """Config 4 (4096 texts of 1 KiB..4 MiB) or 20,000 short texts in one
-    batched build, and the per-text loop beside it."""
+def measure_batch(args, torch, ctx, dev, dist, world, rank, texts, steps, warmup, tune=True, plain_texts=0,
+                  e2e_steps=3, base_sched=None, cpu=True):
+    """Batched build of `texts` (this rank's share by LPT): device-resident
+    suffixes/s over `steps` timed builds, the schedule chosen by the
+    autotuner (coordinate descent over chunk size, tile shape, block shape,
+    finish_below and engine, psacak_b200.autotune), the per-text loop
+    ("plain"), the end-to-end form through psacak8_batch with pageable
+    per-text host buffers, and the roofline of the dominant kernel."""
     import ctypes
-    import torch
     import psacak_b200 as pk
+    from psacak_b200 import autotune
     from psacak_b200 import batch as pb
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = _dist_init(torch, world, local)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if args.workload == "short20k":
-        texts = pb.batch_texts(count=20000, lo=256, hi=8 << 10, seed=args.seed)
-    else:
-        texts = pb.batch_texts(count=4096, seed=args.seed)
     lens = [t.size for t in texts]
     total_all = sum(lens)
     mine = pb.shard_lpt(lens, world)[rank]
     my_texts = [texts[i] for i in mine]
     buf, off = pb.pack(my_texts)
     n = int(buf.size)
-    ctx = pk.Context(local)
-    sched = {"engine": args.engine}
-    if args.workload == "short20k":
-        # texts below the default prefix-doubling cutoff: each sorted by one CTA in shared memory
-        sched["finish_below"] = 1 << 16
     d_texts = torch.from_numpy(buf).to(dev)
     d_sas = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def build():
-        ctx.psacak8_batch_dev(d_texts.data_ptr(), off, d_sas.data_ptr(), stream.cuda_stream, sched)
+    def build_with(sc):
+        ctx.psacak8_batch_dev(d_texts.data_ptr(), off, d_sas.data_ptr(), stream.cuda_stream, sc)
 
-    for _ in range(args.warmup):
+    # the library's NULL schedule, spelled out (the autotuner's start point)
+    default = {"engine": 1, "tile_items": 8, "scan_ctas_per_sm": 4, "batch_chunk_mib": 3072,
+               "finish_below": 1 << 16}
+    if base_sched:
+        default.update(base_sched)
+    tuned = None
+    sched = dict(default)
+    if tune:
+        t0 = time.perf_counter()
+        best, best_ms, table = autotune.coordinate_descent(autotune.device_timer(build_with), default)
+        tuned = {"schedule": best, "ms": best_ms,
+                 "default_ms": next(r["ms"] for r in table if r["schedule"] == default),
+                 "evaluated": len(table), "seconds": time.perf_counter() - t0,
+                 "search": "coordinate descent, one sweep over " + ", ".join(autotune.BATCH_ORDER)}
+        sched = best
+
+    def build():
+        build_with(sched)
+
+    for _ in range(warmup):
         build()
     torch.cuda.synchronize(dev)
     verified = None
@@ -573,7 +668,7 @@ def run_batch(args):
                                                stream.cuda_stream):
                 verified = False
                 break
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(dev.index or 0)
     clocks.start()
     time.sleep(0.3)
     if dist:
@@ -583,26 +678,26 @@ def run_batch(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         build()
     e1.record(stream)
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    launches = (ctx.kernel_launches() - l0) // max(args.steps, 1)
-    ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+    launches = (ctx.kernel_launches() - l0) // max(steps, 1)
+    ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / steps)
     value = total_all / (ms / 1000.0)
     roofline, stats = _profile_roofline(ctx, build, torch, dev)
 
-    # plain: the same texts, one psacak8_dev call each
-    k_plain = len(my_texts) if args.plain_texts <= 0 else min(args.plain_texts, len(my_texts))
+    # plain: the same texts, one psacak8_dev call each (library default schedule)
+    k_plain = len(my_texts) if plain_texts <= 0 else min(plain_texts, len(my_texts))
     torch.cuda.synchronize(dev)
     p0 = time.perf_counter()
     for i in range(k_plain):
         a, b = int(off[i]), int(off[i + 1])
         if b > a:
-            ctx.psacak8_dev(d_texts.data_ptr() + a, b - a, d_sas.data_ptr() + 4 * a, stream.cuda_stream, sched)
+            ctx.psacak8_dev(d_texts.data_ptr() + a, b - a, d_sas.data_ptr() + 4 * a, stream.cuda_stream, None)
     torch.cuda.synchronize(dev)
     plain_s = time.perf_counter() - p0
     plain_value = sum(int(off[i + 1] - off[i]) for i in range(k_plain)) / plain_s
@@ -614,7 +709,7 @@ def run_batch(args):
         ptrs_s = (ctypes.c_void_p * len(my_texts))(*[x.ctypes.data for x in h_sas])
         lens_c = (ctypes.c_uint64 * len(my_texts))(*[t.size for t in my_texts])
         times = []
-        for i in range(max(args.warmup, 1) + args.e2e_steps):  # the same warm-up as the device-resident steps
+        for i in range(max(warmup, 1) + e2e_steps):  # the same warm-up as the device-resident steps
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
@@ -622,13 +717,18 @@ def run_batch(args):
             dt = time.perf_counter() - t0
             if rc != 0:
                 pk._raise(rc)
-            if i >= max(args.warmup, 1):
+            if i >= max(warmup, 1):
                 times.append(dt)
         e2e_s = _max_over_ranks(torch, dist, dev, float(np.mean(times)))
         e2e = {"value": total_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n, "d2h_bytes_per_step": 4 * n,
                "ms_per_step": 1000.0 * e2e_s, "api": "psacak8_batch (host pointers, pageable per-text buffers)"}
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+        if not args.no_verify:
+            # the host arrays must equal the checked device-resident ones
+            dev_sa = d_sas.cpu().numpy().view(np.uint32)
+            e2e["verified"] = bool(verified) and all(
+                np.array_equal(h_sas[i], dev_sa[int(off[i]):int(off[i + 1])]) for i in range(len(my_texts)))
+    cpu_line = None
+    if cpu and rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib
         t0 = time.perf_counter()
@@ -639,17 +739,48 @@ def run_batch(args):
             if time.perf_counter() - t0 > 5.0:
                 break
         dt = time.perf_counter() - t0
-        cpu = {"value": done / dt, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": "oracle builds of the first %d bytes of the batch, text by text" % done}
+        cpu_line = {"value": done / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                    "sample": "oracle builds of the first %d bytes of the batch, text by text" % done}
+    del d_texts, d_sas
+    return {"value": value, "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "texts": len(texts), "total_bytes": total_all, "schedule": sched, "autotune": tuned,
+            "e2e": e2e, "roofline": roofline,
+            "plain": {"value": plain_value, "unit": UNIT, "texts": k_plain,
+                      "api": "psacak8_dev per text, same device-resident texts, library default schedule"},
+            "batched_over_plain": value / plain_value, "cpu_baseline": cpu_line, "clocks": clk,
+            "gpu_launches": int(launches), "verified": verified}
+
+
+def run_batch(args):
+    """Config 4 (4096 texts of 1 KiB..4 MiB) or 20,000 short texts in one
+    batched build, and the per-text loop beside it."""
+    import torch
+    import psacak_b200 as pk
+    from psacak_b200 import batch as pb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = _dist_init(torch, world, local)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    base = {"engine": args.engine} if args.engine else {}
+    if args.workload == "short20k":
+        texts = pb.batch_texts(count=20000, lo=256, hi=8 << 10, seed=args.seed)
+        # texts below the default prefix-doubling cutoff: each sorted by one CTA in shared memory
+        base["finish_below"] = 1 << 16
+    else:
+        texts = pb.batch_texts(count=4096, seed=args.seed)
+    ctx = pk.Context(local)
+    r = measure_batch(args, torch, ctx, dev, dist, world, rank, texts, args.steps, args.warmup,
+                      tune=not args.no_tune, plain_texts=args.plain_texts, e2e_steps=args.e2e_steps,
+                      base_sched=base)
     if rank == 0:
-        line = {"metric": METRIC + " -- batched", "value": value, "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-                "scaling": "strong", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-                "config": workload_config(args), "e2e": e2e, "roofline": roofline,
-                "plain": {"value": plain_value, "unit": UNIT, "texts": k_plain,
-                          "api": "psacak8_dev per text, same device-resident texts"},
-                "batched_over_plain": value / plain_value, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": int(launches), "verified": verified, "total_bytes": total_all}
+        line = {"metric": METRIC + " -- batched", "value": r["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic", "config": workload_config(args)}
+        line.update({k: v for k, v in r.items() if k not in ("value", "unit", "ms_per_step", "steps", "warmup")})
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
@@ -684,16 +815,32 @@ def run_derived(args):
     lcp = torch.empty(n, dtype=torch.int32, device=dev)
     isa = torch.empty(n, dtype=torch.int32, device=dev)
     bwt = torch.empty(n, dtype=torch.uint8, device=dev)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    fm = torch.empty(pk.fm_bytes(n), dtype=torch.uint8, device=dev)
+    # FM-index queries: 2^20 patterns of 20 bytes, half taken from the text
+    # (they occur), half random over ACGT
+    qn, qm = 1 << 20, 20
+    qrng = np.random.default_rng(args.seed + 3)
+    qpos = qrng.integers(0, n - qm, qn // 2)
+    pats = np.concatenate([text[(qpos[:, None] + np.arange(qm)[None, :])].reshape(-1),
+                           np.frombuffer(b"ACGT", np.uint8)[qrng.integers(0, 4, (qn - qn // 2) * qm)]])
+    dpat = torch.from_numpy(pats).to(dev)
+    doff = torch.arange(0, (qn + 1) * qm, qm, dtype=torch.int64, device=dev)
+    dranges = torch.empty(2 * qn, dtype=torch.int32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    primary = [0]
 
     def step():
         ev[0].record(stream)
         ctx.lcp8_dev(dt.data_ptr(), n, ds.data_ptr(), lcp.data_ptr(), s)
         ev[1].record(stream)
-        ctx.bwt8_dev(dt.data_ptr(), n, ds.data_ptr(), bwt.data_ptr(), s)
+        primary[0] = ctx.bwt8_dev(dt.data_ptr(), n, ds.data_ptr(), bwt.data_ptr(), s)
         ev[2].record(stream)
         ctx.isa_dev(ds.data_ptr(), n, isa.data_ptr(), s)
         ev[3].record(stream)
+        ctx.fm_build_dev(bwt.data_ptr(), n, primary[0], fm.data_ptr(), s)
+        ev[4].record(stream)
+        ctx.fm_count_dev(fm.data_ptr(), bwt.data_ptr(), dpat.data_ptr(), doff.data_ptr(), qn, dranges.data_ptr(), s)
+        ev[5].record(stream)
 
     for _ in range(args.warmup):
         step()
@@ -702,13 +849,15 @@ def run_derived(args):
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    tl = tb = ti = 0.0
+    tl = tb = ti = tf = tq = 0.0
     for _ in range(args.steps):
         step()
         torch.cuda.synchronize(dev)
         tl += ev[0].elapsed_time(ev[1])
         tb += ev[1].elapsed_time(ev[2])
         ti += ev[2].elapsed_time(ev[3])
+        tf += ev[3].elapsed_time(ev[4])
+        tq += ev[4].elapsed_time(ev[5])
     clk = clocks.stop()
     ms = (tl + tb + ti) / args.steps
     if dist:
@@ -733,6 +882,15 @@ def run_derived(args):
         want_b, want_p = oracle_lib.bwt(tp, sap)
         verified = bool(sa_ok and (lp.cpu().numpy().view(np.uint32) == oracle_lib.lcp(tp, sap)).all()
                         and prim == want_p and (bp.cpu().numpy() == want_b).all())
+        # FM-index ranges of 64 of the full text's queries against binary
+        # search on the full suffix array (host copy)
+        sa_full = ds.cpu().numpy().view(np.uint32)
+        rg = dranges.cpu().numpy().view(np.uint32).reshape(-1, 2)
+        for q in list(range(0, qn, qn // 32)) + list(range(qn // 2, qn, qn // 32)):
+            want = oracle_lib.sa_range8(text, sa_full, pats[q * qm:(q + 1) * qm])
+            got = (int(rg[q, 0]), int(rg[q, 1]))
+            if (want[1] > want[0] and got != want) or (want[1] == want[0] and got[1] != got[0]):
+                verified = False
     if rank == 0:
         line = {
             "metric": "suffixes/sec (LCP array + BWT + inverse SA from a suffix array, bit-exact)",
@@ -740,9 +898,15 @@ def run_derived(args):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8/u32", "data": "synthetic", "config": workload_config(args),
             "per_array_ms": {"lcp": tl / args.steps, "bwt": tb / args.steps, "isa": ti / args.steps},
+            "fm_index": {"build_ms": tf / args.steps, "build_gbs_algorithmic": 3.0 * n / (tf / args.steps) / 1e6,
+                         "queries": qn, "pattern_bytes": qm, "count_ms": tq / args.steps,
+                         "patterns_per_s": qn / (tq / args.steps / 1000.0),
+                         "index_bytes": pk.fm_bytes(n),
+                         "note": "build reads the BWT (n bytes) and writes the rank checkpoints (~2n bytes); a "
+                                 "query is a backward search, one warp per pattern, 2 rank lookups per byte"},
             "clocks": clk, "verified": verified,
             "verification": "device SA check of the full text; LCP and BWT of its 64 MiB prefix equal to the CPU "
-                            "restatements",
+                            "restatements; 64 FM-index query ranges equal to binary search on the suffix array",
         }
         print(json.dumps(line), flush=True)
     ctx.close()

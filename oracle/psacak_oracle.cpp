@@ -21,11 +21,18 @@
 
 #include <algorithm>
 #include <cstring>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
 #include <map>
 #include <vector>
 
 /* The pipelined scans of the reference's par_induce_sort (psacak_oracle_par.cpp). */
 namespace oracle_par {
+void induce_sort32_par(const uint32_t *text, uint32_t *suf, size_t len, bool left_most, unsigned threads);
+size_t name_chunks_par(uint32_t *lmssubs, size_t n, uint32_t *work, size_t wlen, unsigned threads,
+                       const std::function<bool(size_t, size_t)> &differs);
 void induce_sort8_par(const uint8_t *text, size_t len, uint32_t *suf, uint32_t *ptrs_head, uint32_t *ptrs_tail,
                       bool left_most, unsigned threads);
 }
@@ -238,11 +245,34 @@ void translate(uint32_t *t, size_t n, const uint32_t *tails) {
  * in suf[..n], leaves the translated reduced string in the tail of suf and
  * the bucket tails in suf[..k]; returns k. */
 template <class C>
-size_t name_lmssubstrings(const C *text, size_t len, uint32_t *suf, size_t n) {
+size_t name_lmssubstrings(const C *text, size_t len, uint32_t *suf, size_t n, unsigned threads = 0) {
     if (n == 0) return 0;
     uint32_t *lmssubs = suf;
     uint32_t *work = suf + n;
     size_t wlen = len - n;
+    if (threads > 1 && n >= (1u << 16)) {
+        /* src/naming.rs:169-259 fastpar naming: flags and names by chunks in
+         * parallel (psacak_oracle_par.cpp), bucket tails serially */
+        oracle_par::name_chunks_par(lmssubs, n, work, wlen, threads, [&](size_t i0, size_t i1) {
+            return !fp_equals(text, len, i0, fp_get(text, len, i0), i1, fp_get(text, len, i1));
+        });
+        size_t k = 0, h = 0, m = 0;
+        for (size_t i = 0; i < n; i++) {
+            if (lmssubs[i] & (1u << 31)) {
+                lmssubs[k] = (uint32_t)(h + m);
+                k++;
+                h += m;
+                m = 0;
+            }
+            m++;
+        }
+        lmssubs[k] = (uint32_t)(h + m);
+        k++;
+        size_t p = wlen - n;
+        compact_right(work, wlen, UINT32_MAX);
+        translate(work + p, n, lmssubs);
+        return k;
+    }
     size_t k = 0, h = 0, m = 1;
     size_t i0 = lmssubs[0];
     Fingerprint<C> fp0 = fp_get(text, len, i0);
@@ -443,27 +473,32 @@ void induce_sort32(const uint32_t *text, uint32_t *suf, size_t len, bool left_mo
 
 /* src/psacak32.rs:24-56 psacak32: one inner level on bucket-pointer text. */
 void psacak32_level(const uint32_t *text, uint32_t *suf, size_t len, uint32_t level,
-                    Trace *tr) {
+                    Trace *tr, unsigned threads = 0) {
+    /* with threads: the pipelined scans (src/psacak32.rs:289-484) from two
+     * blocks of 64Ki up, the parallel naming */
+    const bool par = threads > 1 && len >= 2 * 64 * 1024;
     if (len <= 3) {
         saca_tiny(text, len, suf);
         trace_push(tr, level, 4, len, 0, 0, 0);
         return;
     }
     put_lmscharacters32(text, suf, len);
-    induce_sort32(text, suf, len, true);
+    if (par) oracle_par::induce_sort32_par(text, suf, len, true, threads);
+    else induce_sort32(text, suf, len, true);
     size_t n = compact_left_range(suf, len, 1, EMPTY - 1);
-    size_t k = name_lmssubstrings(text, len, suf, n);
+    size_t k = name_lmssubstrings(text, len, suf, n, threads);
     uint32_t *suf1 = suf;
     uint32_t *text1 = suf + (len - n);
     trace_push(tr, level, 4, len, n, k, k < n ? oracle_hash_u32(text1, n) : 0);
     if (k < n) {
-        psacak32_level(text1, suf1, n, level + 1, tr);
+        psacak32_level(text1, suf1, n, level + 1, tr, threads);
     } else {
         for (size_t i = 0; i < n; i++) suf1[text1[i]] = (uint32_t)i;
     }
     permutate_lmssuffixes(text, len, suf, n);
     put_lmssuffixes32(text, len, suf, n);
-    induce_sort32(text, suf, len, false);
+    if (par) oracle_par::induce_sort32_par(text, suf, len, false, threads);
+    else induce_sort32(text, suf, len, false);
 }
 
 /* ---------------------------------------------------------------------- */
@@ -588,6 +623,22 @@ void induce_sort8_any(const uint8_t *text, size_t len, uint32_t *suf, Buckets &b
     else induce_sort8(text, len, suf, bkt, left_most);
 }
 
+/* PSACAK_ORACLE_TIMES=1: wall time of each stage on stderr (for sizing the
+ * CPU baselines; no effect on results). */
+static void stage_mark(const char *what) {
+    static int on = -1;
+    static std::chrono::steady_clock::time_point last;
+    if (on < 0) {
+        const char *e = getenv("PSACAK_ORACLE_TIMES");
+        on = e && e[0] == '1';
+        last = std::chrono::steady_clock::now();
+    }
+    if (!on) return;
+    auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "[oracle] %-28s %8.3f s\n", what, std::chrono::duration<double>(now - last).count());
+    last = now;
+}
+
 /* src/psacak8.rs:19-53 psacak8. */
 void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr, unsigned threads = 0) {
     if (len <= 3) {
@@ -595,12 +646,16 @@ void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr, uns
         trace_push(tr, 0, 1, len, 0, 0, 0);
         return;
     }
+    stage_mark("start");
     Buckets bkt;
     bkt.build(text, len);
     put_lmscharacters8(text, len, suf, bkt);
+    stage_mark("typing+placement");
     induce_sort8_any(text, len, suf, bkt, true, threads);
+    stage_mark("induce lms-substrings");
     size_t n = compact_left(suf, len, 0);
-    size_t k = name_lmssubstrings(text, len, suf, n);
+    size_t k = name_lmssubstrings(text, len, suf, n, threads);
+    stage_mark("compact+naming");
     uint32_t *suf1 = suf;
     uint32_t *text1 = suf + (len - n);
     trace_push(tr, 0, 1, len, n, k, k < n ? oracle_hash_u32(text1, n) : 0);
@@ -612,13 +667,16 @@ void psacak8_impl(const uint8_t *text, size_t len, uint32_t *suf, Trace *tr, uns
     }
     if (tr && tr->stop_after_level0) return;
     if (k < n) {
-        psacak32_level(text1, suf1, n, 1, tr);
+        psacak32_level(text1, suf1, n, 1, tr, threads);
     } else {
         for (size_t i = 0; i < n; i++) suf1[text1[i]] = (uint32_t)i;
     }
+    stage_mark("inner levels");
     permutate_lmssuffixes(text, len, suf, n);
     put_lmssuffixes8(suf, len, bkt, n);
+    stage_mark("permute+put");
     induce_sort8_any(text, len, suf, bkt, false, threads);
+    stage_mark("final induce");
 }
 
 /* src/psacak32.rs:912-943 translate_sample: ordered histogram, L -> bucket
@@ -766,6 +824,36 @@ uint64_t oracle_bwt8(const uint8_t *text, uint64_t n, const uint32_t *sa, uint8_
         else bwt[o++] = text[sa[i] - 1];
     }
     return primary;
+}
+
+/* Suffix-array indices [lo, hi) whose suffixes start with pat[0, m): two
+ * binary searches on the suffix array comparing suffixes with the pattern
+ * (a suffix that ends inside the pattern's length while equal so far sorts
+ * before it).  The independent check of the FM-index's backward search. */
+static int cmp_prefix(const uint8_t *text, uint64_t n, uint64_t p, const uint8_t *pat, uint64_t m) {
+    for (uint64_t k = 0; k < m; k++) {
+        if (p + k >= n) return -1;
+        if (text[p + k] != pat[k]) return text[p + k] < pat[k] ? -1 : 1;
+    }
+    return 0;
+}
+
+void oracle_sa_range8(const uint8_t *text, uint64_t n, const uint32_t *sa, const uint8_t *pat, uint64_t m,
+                      uint64_t *lo, uint64_t *hi) {
+    uint64_t a = 0, b = n;  // first index with cmp >= 0
+    while (a < b) {
+        uint64_t mid = a + (b - a) / 2;
+        if (cmp_prefix(text, n, sa[mid], pat, m) < 0) a = mid + 1;
+        else b = mid;
+    }
+    uint64_t c = a, d = n;  // first index with cmp > 0
+    while (c < d) {
+        uint64_t mid = c + (d - c) / 2;
+        if (cmp_prefix(text, n, sa[mid], pat, m) <= 0) c = mid + 1;
+        else d = mid;
+    }
+    *lo = a;
+    *hi = c;
 }
 
 uint64_t oracle_reduced8(const uint8_t *text, uint64_t n, uint32_t *out, uint64_t cap,

@@ -24,12 +24,21 @@ from . import lib, _raise, _sched_ptr, ENGINE_BUCKET, ENGINE_DOUBLING
 NF = 16
 NH = 64
 
+# Recursion strategy is the knob whose best value depends on the text: prefix
+# doubling needs log2(longest repeat) rounds over every unresolved suffix, so
+# it wins on repeat-poor texts of any length and loses on repetitive ones,
+# where induced sorting and recursion win.  0 = never, ALWAYS = the whole
+# text is sorted by prefix doubling.
+ALWAYS = 0xFFFFFFFF
+FINISH_GRID = [0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, 1 << 24, 1 << 26, ALWAYS]
 SCHEDULES = [
-    {"engine": e, "inner_engine": ENGINE_DOUBLING, "tile_items": t, "finish_below": f}
-    for e in (ENGINE_BUCKET, ENGINE_DOUBLING) for t in (8, 12, 16) for f in (0, 1 << 16, 1 << 20, 1 << 24)
+    {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": t, "finish_below": f}
+    for t in (8, 16) for f in FINISH_GRID
 ]
-DEFAULT_INDEX = SCHEDULES.index({"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 8,
-                                 "finish_below": 0})
+# The schedule a NULL psacak_schedule stands for (include/psacak_b200.h).
+LIBRARY_DEFAULT = {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 8,
+                   "finish_below": 1 << 16}
+DEFAULT_INDEX = SCHEDULES.index(LIBRARY_DEFAULT)
 
 
 def _bind():
@@ -85,7 +94,7 @@ def build(ctx, d_text, n, width, d_sa, stream, schedule):
 
 def autotune(ctx, d_text, n, width, d_sa, reps=2, schedules=SCHEDULES):
     """Device milliseconds of every schedule on one text (min over reps,
-    after one warm-up build)."""
+    after one warm-up build); a None schedule is the library default."""
     import torch
     stream = torch.cuda.current_stream()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -122,6 +131,13 @@ class Selector:
                 o += w.size + fan_out  # biases stay 0
             params = p
         self.params = torch.from_numpy(np.asarray(params, dtype=np.float32).copy()).cuda()
+
+    def bind(self, ctx):
+        """The same network (parameters shared, not copied) driven through
+        another context, e.g. one per serving thread."""
+        other = object.__new__(Selector)
+        other.ctx, other.k, other.np, other.params = ctx, self.k, self.np, self.params
+        return other
 
     def _ptr(self, t):
         return ctypes.c_void_p(t.data_ptr())
@@ -182,7 +198,11 @@ class Selector:
 
     @classmethod
     def load(cls, ctx, path):
+        """The saved network, or None when it was trained for another
+        schedule list than SCHEDULES (its outputs would not index it)."""
         d = np.load(path, allow_pickle=False)
+        if "schedules" not in d.files or json.loads(str(d["schedules"])) != SCHEDULES:
+            return None
         return cls(ctx, k=int(d["k"]), params=d["params"])
 
 

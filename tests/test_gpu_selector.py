@@ -1,6 +1,6 @@
 """The schedule selector on the GPU: forward and backward kernels against the
 CPU fp32 reference (tolerance rtol 1e-3 / atol 1e-5), training, inference,
-statistics, and the gain of the trained network over the fixed default
+statistics, and the gain of the trained network over the best fixed
 schedule on held-out texts (every schedule gives the same SA)."""
 import numpy as np
 import pytest
@@ -68,47 +68,59 @@ def test_text_statistics(ctx):
     assert fr[6] > f[6]               # repeats are seen
 
 
-def test_selector_gains_over_default_schedule(ctx):
-    """Train on autotuned timings of training texts, then compare the picks
-    with the fixed default schedule on held-out texts."""
+def test_selector_beats_the_best_fixed_schedule(ctx):
+    """What the trained network gains over the method without it.  Two kinds
+    of text want opposite recursion strategies: repeat-poor i.i.d. texts are
+    fastest sorted directly by prefix doubling (few rounds), texts made of
+    a block repeated many times are fastest by induced sorting (prefix
+    doubling needs log2 of the repeat length in rounds over every suffix).
+    No fixed schedule suits both, so the best fixed schedule (the one with
+    the smallest total time on the training texts) loses on one kind; the
+    network, reading the sampled repeat rate, picks per text.  Held-out
+    texts: the selector's total time must be below the best fixed
+    schedule's by at least 10%, and every pick builds the oracle's SA."""
     rng = np.random.default_rng(5)
 
     def texts(count, seed):
         out = []
         for i in range(count):
-            n = int(np.exp(rng.uniform(np.log(8 << 10), np.log(2 << 20))))
+            n = int(np.exp(rng.uniform(np.log(1 << 20), np.log(6 << 20))))
             if i % 2 == 0:
-                out.append((synth.genome(n, seed=seed + i), 1))
+                out.append((synth.iid(n, b"ACGT", seed=seed + i), 1))
             else:
-                out.append((synth.zipf32(n // 4 + 16, alphabet=1 << 16, repeat_frac=0.0, seed=seed + i), 4))
+                block = synth.iid(int(rng.integers(2000, 9000)), b"ACGT", seed=seed + i)
+                t = np.resize(block, n)
+                t[rng.integers(0, n, 8)] = ord("N")  # a few mutations, so the repeats are not exact to the end
+                out.append((t, 1))
         return out
 
     def measure(items):
         X, Tm = [], []
         for t, w in items:
-            d = torch.from_numpy(t.view(np.int32) if w == 4 else t).cuda()
+            d = torch.from_numpy(t).cuda()
             sa = torch.empty(t.size, dtype=torch.int32, device="cuda")
             X.append(sel.features(ctx, d.data_ptr(), t.size, w))
             Tm.append(sel.autotune(ctx, d.data_ptr(), t.size, w, sa.data_ptr(), reps=2))
         return np.array(X), np.array(Tm)
 
     Xtr, Ttr = measure(texts(24, 100))
-    Xte, Tte = measure(texts(10, 900))
+    Xte, Tte = measure(texts(12, 900))
+    best_fixed = int(np.argmin(Ttr.sum(axis=0)))
     T, M = sel.targets(Ttr)
-    net = sel.Selector(ctx, seed=6)
+    net = sel.Selector(ctx, k=len(sel.SCHEDULES), seed=6)
     net.train(Xtr, T, M, epochs=1500, lr=3e-3)
     picks = [net.predict(x)[0] for x in Xte]
     sel_ms = sum(Tte[i, p] for i, p in enumerate(picks))
-    def_ms = Tte[:, sel.DEFAULT_INDEX].sum()
+    fixed_ms = Tte[:, best_fixed].sum()
     best_ms = Tte.min(axis=1).sum()
-    print("held-out: best %.2f ms, selector %.2f ms, default %.2f ms" % (best_ms, sel_ms, def_ms))
-    assert sel_ms <= def_ms * 1.02
-    # a picked schedule still builds the oracle's suffix array
-    t, w = texts(1, 7000)[0]
-    d = torch.from_numpy(t.view(np.int32) if w == 4 else t).cuda()
-    sa = torch.empty(t.size, dtype=torch.int32, device="cuda")
-    c, _ = net.predict(sel.features(ctx, d.data_ptr(), t.size, w))
-    sel.build(ctx, d.data_ptr(), t.size, w, sa.data_ptr(), 0, sel.SCHEDULES[c])
-    torch.cuda.synchronize()
-    want = o.psacak8(t) if w == 1 else o.psacak32(t)
-    assert (sa.cpu().numpy().view(np.uint32) == want).all()
+    print("held-out: per-text best %.2f ms, selector %.2f ms, best fixed (%s) %.2f ms"
+          % (best_ms, sel_ms, sel.SCHEDULES[best_fixed], fixed_ms))
+    assert sel_ms <= 0.9 * fixed_ms
+    # every picked schedule builds the oracle's suffix array
+    for t, w in texts(4, 7000):
+        d = torch.from_numpy(t).cuda()
+        sa = torch.empty(t.size, dtype=torch.int32, device="cuda")
+        p, _ = net.predict(sel.features(ctx, d.data_ptr(), t.size, w))
+        sel.build(ctx, d.data_ptr(), t.size, w, sa.data_ptr(), 0, sel.SCHEDULES[p])
+        torch.cuda.synchronize()
+        assert (sa.cpu().numpy().view(np.uint32) == o.psacak8(t)).all()

@@ -129,10 +129,13 @@ def test_synthetic_traces_pinned():
 
 @pytest.mark.parametrize("threads", [1, 3, 8])
 def test_pipelined_scans_equal_serial(threads):
-    """The restatement of the reference's pipelined induced scans (the
-    all-core CPU baseline) builds the same suffix array as the serial
-    restatement: texts of several 128Ki blocks, with repeats, runs and an
-    all-equal stretch that sends writes far beyond the next block."""
+    """The all-core CPU baseline -- the restatement of the reference's
+    pipelined induced scans, its chunked parallel naming and the prefetching
+    u32 scans of the inner levels -- builds the same suffix array as the
+    serial restatement: texts of several 128Ki blocks (their reduced strings
+    pass 2 x 64Ki symbols and 2^16 LMS substrings, so the inner levels and
+    the naming run in parallel too), with repeats, runs and an all-equal
+    stretch that sends writes far beyond the next block."""
     from psacak_b200 import synth
     rng = np.random.default_rng(threads)
     texts = [synth.genome(3 << 20, seed=threads),
