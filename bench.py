@@ -388,6 +388,7 @@ def run_b200(args):
         dist.barrier()
     torch.cuda.synchronize(dev)
     l0 = ctx.kernel_launches()
+    rt0 = ctx.round_trips()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     if flush is None:
@@ -411,6 +412,7 @@ def run_b200(args):
     if dist:
         dist.barrier()
     launches = (ctx.kernel_launches() - l0) // max(args.steps, 1)
+    round_trips = (ctx.round_trips() - rt0) // max(args.steps, 1)
     clk = clocks.stop()
     ms = step_ms_total / args.steps
     if dist:
@@ -564,6 +566,7 @@ def run_b200(args):
             "hbm_gbs_algorithmic_build": build_gbs,
             "build_algorithmic_bytes": build_bytes,
             "cpu_baseline": cpu, "cpu_baseline_all_cores": cpu_all, "clocks": clk, "gpu_launches": int(launches),
+            "host_round_trips_per_step": int(round_trips),
             "verified": verified, "levels": [[lv["m"], lv["n_lms"], lv["k"]] for lv in trace],
         }
         print(json.dumps(line), flush=True)

@@ -261,8 +261,14 @@ PSACAK_API int psacak_fm_count_dev(psacak_ctx *ctx, const void *d_fm, const uint
                                    const uint8_t *d_patterns, const uint64_t *d_offsets, uint32_t n_patterns,
                                    uint32_t *d_ranges, void *stream);
 
-/* Number of kernels the library launched since the context was created. */
+/* Number of kernels the library launched (all contexts of the process). */
 PSACAK_API uint64_t psacak_kernel_launches(psacak_ctx *ctx);
+
+/* Number of host round trips inside builds (all contexts of the process):
+ * times the host waited for a count or histogram computed on the device
+ * before it could choose the next launches.  They set the latency floor of
+ * short and mid-size builds. */
+PSACAK_API uint64_t psacak_round_trips(psacak_ctx *ctx);
 
 #ifdef __cplusplus
 }

@@ -131,6 +131,8 @@ def lib():
         L.psacak_check_sa8_noalloc.restype = i32
         L.psacak_kernel_launches.argtypes = [p]
         L.psacak_kernel_launches.restype = u64
+        L.psacak_round_trips.argtypes = [p]
+        L.psacak_round_trips.restype = u64
         L.psacak_isa_dev.argtypes = [p, p, u64, p, p]
         L.psacak_bwt8_dev.argtypes = [p, p, u64, p, p, ctypes.POINTER(u64), p]
         L.psacak_lcp8_dev.argtypes = [p, p, u64, p, p, p]
@@ -306,6 +308,10 @@ class Context:
 
     def kernel_launches(self):
         return int(lib().psacak_kernel_launches(self._h))
+
+    def round_trips(self):
+        """Host round trips (device counts read back mid-build) so far."""
+        return int(lib().psacak_round_trips(self._h))
 
     def profile(self, on=True):
         _raise(lib().psacak_profile_enable(self._h, 1 if on else 0))

@@ -107,15 +107,27 @@ static inline uint32_t grid_for(uint64_t n, uint32_t cap = 16384) {
     return (uint32_t)(g < cap ? g : cap);
 }
 
-static status_t hash_device(Ctx &ctx, const uint32_t *v, uint64_t n, uint64_t *out) {
-    unsigned long long *d = (unsigned long long *)(ctx.d_scalars + 32);
+static void trace_push(Ctx &ctx, uint32_t level, uint32_t width, uint64_t m, uint64_t n1, uint64_t k, uint64_t hash);
+
+// Hash of the reduced string handed to the next level, for the trace:
+// computed into the level's slot of ctx.d_hashes and read back with the
+// others after the build (Ctx::resolve_trace), so it costs no round trip.
+static status_t trace_push_hashed(Ctx &ctx, uint32_t level, uint32_t width, uint64_t m, uint64_t n1, uint64_t k,
+                                  const uint32_t *v) {
+    const uint32_t slot = (uint32_t)ctx.pending_hash.size();
+    unsigned long long *d = slot < Ctx::HASH_SLOTS ? ctx.d_hashes + slot : (unsigned long long *)(ctx.d_scalars + 32);
     PSK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx.stream));
-    k_hash_u32<<<grid_for(n, 2048), 256, 0, ctx.stream>>>(v, n, d);
+    k_hash_u32<<<grid_for(n1, 2048), 256, 0, ctx.stream>>>(v, n1, d);
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
-    uint32_t h[2];
+    if (slot < Ctx::HASH_SLOTS) {
+        trace_push(ctx, level, width, m, n1, k, 0);
+        ctx.pending_hash.push_back({ctx.trace.size() - 1, slot});
+        return PSACAK_OK;
+    }
+    uint32_t h[2];  // deeper than the slots: read now
     PSK_TRY(ctx.read_u32((const uint32_t *)d, h, 2));
-    *out = ((uint64_t)h[1] << 32) | h[0];
+    trace_push(ctx, level, width, m, n1, k, ((uint64_t)h[1] << 32) | h[0]);
     return PSACAK_OK;
 }
 
@@ -215,6 +227,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     if constexpr (sizeof(C) == 1) {
         ByteHist hh;
         PSK_CUDA(cudaMemcpyAsync(&hh, hist.get(), sizeof(ByteHist), cudaMemcpyDeviceToHost, s));
+        PSK_ROUND_TRIP();
         PSK_TRY(ctx.sync());
         uint32_t acc = 0, lacc = 0;
         for (int c = 0; c < 256; c++) {
@@ -327,9 +340,7 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
                 ctx.debug_k = k;
                 return ctx.sync();
             }
-            uint64_t hsh = 0;
-            PSK_TRY(hash_device(ctx, red, n1, &hsh));
-            trace_push(ctx, level, width, n, n1, k, hsh);
+            PSK_TRY(trace_push_hashed(ctx, level, width, n, n1, k, red));
             ctx.mark("translate", level);
             // heads[c] (c <= k) are the next level's bucket boundaries by name
             PSK_TRY(build_level<uint32_t>(ctx, red, names1, heads, k, n1, sa1, level + 1));
@@ -567,6 +578,7 @@ status_t ctx_init(Ctx &c, int device) {
     // error word + wait-limit override (common.cuh)
     PSK_CUDA(cudaMalloc(&c.d_err, 2 * sizeof(uint32_t)));
     PSK_CUDA(cudaMemset(c.d_err, 0, 2 * sizeof(uint32_t)));
+    PSK_CUDA(cudaMalloc(&c.d_hashes, Ctx::HASH_SLOTS * sizeof(unsigned long long)));
     PSK_CUDA(cudaMalloc(&c.d_induced, 2 * sizeof(unsigned long long)));
     PSK_CUDA(cudaMemset(c.d_induced, 0, 2 * sizeof(unsigned long long)));
     c.scan_ctas = 4 * (uint32_t)c.dev.num_sms;
@@ -593,6 +605,8 @@ void ctx_free(Ctx &c) {
     if (c.d_scalars) cudaFree(c.d_scalars);
     if (c.d_err) cudaFree(c.d_err);
     if (c.d_induced) cudaFree(c.d_induced);
+    if (c.d_hashes) cudaFree(c.d_hashes);
+    c.d_hashes = nullptr;
     if (c.arena) cudaFree(c.arena);
     c.arena = nullptr;
     if (c.own_stream) cudaStreamSynchronize(c.own_stream);
@@ -654,6 +668,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     c.stream = stream ? stream : c.own_stream;
     apply_schedule(c, sched);
     c.trace.clear();
+    c.pending_hash.clear();
     PSK_TRY(c.arena_prepare());
     {
         const char *e = getenv("PSACAK_STAGE_TIMES");
@@ -668,6 +683,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
     c.mark("final induce (level 0)", 0);
     PSK_TRY(c.sync());
     PSK_TRY(c.check_device_error());
+    PSK_TRY(c.resolve_trace());
     PSK_TRY(profile_collect(c));
     return PSACAK_OK;
 }
@@ -955,6 +971,11 @@ uint64_t psacak_kernel_launches(psacak_ctx *ctx) {
     return g_kernel_launches.load();
 }
 
+uint64_t psacak_round_trips(psacak_ctx *ctx) {
+    (void)ctx;
+    return g_round_trips.load();
+}
+
 int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *offsets, uint32_t n_texts,
                       uint32_t *d_sas, void *stream, const psacak_schedule *sched) {
     clear_error();
@@ -968,12 +989,14 @@ int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *o
     c.stream = stream ? (cudaStream_t)stream : c.own_stream;
     apply_schedule(c, sched);
     c.trace.clear();
+    c.pending_hash.clear();
     PSK_TRY(c.arena_prepare());
     ProfGuard pg(c);
     status_t st = build_batch(c, d_texts, offsets, n_texts, d_sas);
     if (st != PSACAK_OK) return c.fail(st);
     PSK_TRY(c.sync());
     PSK_TRY(c.check_device_error());
+    PSK_TRY(c.resolve_trace());
     PSK_TRY(profile_collect(c));
     return PSACAK_OK;
 }
@@ -1151,7 +1174,7 @@ int psacak_debug_stalled_scan(psacak_ctx *ctx, const uint32_t *d_in, uint32_t *d
     PSK_CUDA(cudaMemcpyAsync(ticket, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
     k_lbscan<uint32_t, OpSum<uint32_t>, CopyLoad, CopyStore><<<(uint32_t)(ntiles - 1), LS_BLOCK, 0, c.stream>>>(
         CopyLoad{d_in}, CopyStore{d_out}, n, OpSum<uint32_t>(), c.ss.flags, ticket, c.os.epoch, (uint32_t)ntiles,
-        (uint32_t *)nullptr, c.d_err);
+        (uint32_t *)nullptr, c.d_err, (const uint32_t *)nullptr);
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
     PSK_TRY(c.sync());
@@ -1191,6 +1214,7 @@ int psacak_debug_reduced8(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, ui
     c.stream = c.own_stream;
     apply_schedule(c, sched);
     c.trace.clear();
+    c.pending_hash.clear();
     c.debug_red = d_red;
     c.debug_cap = cap;
     c.debug_n1 = c.debug_k = 0;

@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "hostio.cuh"
@@ -41,6 +42,12 @@ struct Ctx {
     uint32_t *debug_red = nullptr;
     uint64_t debug_cap = 0, debug_n1 = 0, debug_k = 0;
     std::vector<psacak_level_info> trace;
+    // Reduced-string hashes of the trace are computed into d_hashes (one
+    // u64 per level, up to HASH_SLOTS) and read back once, when the build
+    // has finished (resolve_trace), instead of a read-back per level.
+    static constexpr uint32_t HASH_SLOTS = 64;
+    unsigned long long *d_hashes = nullptr;
+    std::vector<std::pair<size_t, uint32_t>> pending_hash;  // (trace index, slot)
     bool profiling = false;
     bool stage_timing = false;  // PSACAK_STAGE_TIMES=1: sync + print wall time per stage
     double stage_t0 = 0;
@@ -217,20 +224,22 @@ struct Ctx {
     }
     ScanEnv scan_env() { return ScanEnv{&ss, &os, d_err}; }
     // Single-pass scan (see lbscan.cuh) over n items.
+    // `dn` (nullable): the item count is on the device, n is its bound.
     template <class T, class Op, class Load, class Store>
-    status_t scan(Load ld, Store st, uint64_t n, T *total_out, Op op, const char *name) {
+    status_t scan(Load ld, Store st, uint64_t n, T *total_out, Op op, const char *name, const uint32_t *dn = nullptr) {
         PSK_TRY(ensure_scan(n));
-        return lb_scan<T, Op>(ld, st, n, total_out, op, ss, os, d_err, stream, name);
+        return lb_scan<T, Op>(ld, st, n, total_out, op, ss, os, d_err, stream, name, dn);
     }
     // Stable LSD radix sort of (key, value) pairs on bits [b0, b1); the
     // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).
     // `hist_ready`: the digits were already counted into d_hist by the
     // keys' producer.
     template <class K, class V>
-    status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1, bool hist_ready = false) {
+    status_t radix_sort(K *k0, V *v0, K *k1, V *v1, uint64_t n, int b0, int b1, int *in1, bool hist_ready = false,
+                        const uint32_t *dn = nullptr) {
         PSK_TRY(ensure_onesweep(ceil_div(n, 8 * OS_BLOCK) + 1));
         return radix_sort_pairs<K, V>(k0, v0, k1, v1, n, b0, b1, d_hist, h_hist, m_hist, os, d_err, in1, stream, RADIX_IPT,
-                                      hist_ready);
+                                      hist_ready, dn);
     }
     // Single-pass stable compaction (see compact1).
     template <class Pred, class Emit>
@@ -240,6 +249,18 @@ struct Ctx {
     }
     status_t sync() {
         PSK_CUDA(cudaStreamSynchronize(stream));
+        return PSACAK_OK;
+    }
+    // Fills in the trace's deferred hashes (one read-back for all levels).
+    status_t resolve_trace() {
+        if (pending_hash.empty()) return PSACAK_OK;
+        uint32_t top = 0;
+        for (auto &ph : pending_hash) top = ph.second + 1 > top ? ph.second + 1 : top;
+        uint32_t h[2 * HASH_SLOTS];
+        PSK_TRY(read_u32((const uint32_t *)d_hashes, h, 2 * top));
+        for (auto &ph : pending_hash)
+            trace[ph.first].hash = ((uint64_t)h[2 * ph.second + 1] << 32) | h[2 * ph.second];
+        pending_hash.clear();
         return PSACAK_OK;
     }
     status_t check_device_error() {

@@ -204,11 +204,13 @@ __global__ void k_group_starts(Geom<C> g, uint64_t nbuckets, uint32_t *gstart) {
 // Keys of one round: (group id, rank of j + h).  The block also counts the
 // digits of every radix pass of the keys (bits [0, nbits)) into `hist`, so
 // the sort needs no histogram pass of its own.
+// `dcnt` (nullable): the item count is on the device, cnt_max bounds it.
 __global__ void __launch_bounds__(256) k_keys(const uint32_t *__restrict__ Wg, const uint32_t *__restrict__ Wv,
-                                              uint64_t cnt, const uint32_t *__restrict__ R, uint64_t n, uint64_t h,
-                                              int KB, uint64_t *keys, uint32_t *vals, int nbits, uint32_t *hist,
-                                              uint32_t *err) {
+                                              uint64_t cnt_max, const uint32_t *dcnt, const uint32_t *__restrict__ R,
+                                              uint64_t n, uint64_t h, int KB, uint64_t *keys, uint32_t *vals,
+                                              int nbits, uint32_t *hist, uint32_t *err) {
     __shared__ uint32_t sh[RADIX_MAX_PASSES * 256];
+    const uint64_t cnt = dcnt ? (*dcnt < cnt_max ? *dcnt : cnt_max) : cnt_max;
     const int npasses = (nbits + 7) / 8;
     for (int i = threadIdx.x; i < npasses * 256; i += blockDim.x) sh[i] = 0;
     __syncthreads();
@@ -260,10 +262,12 @@ struct RoundLoad {
     const uint64_t *keys;
     const uint32_t *vals;
     const uint32_t *gstart;  // group id -> first slot (this round)
-    uint64_t cnt, n, ngroups;
+    uint64_t cnt, n, ngroups;  // ngroups: a bound of the group ids
     int KB;
     uint32_t *err;
+    const uint32_t *dcnt;  // nullable: the item count on the device (cnt bounds it)
     __device__ __forceinline__ Tri operator()(uint64_t i, RoundPayload &pl) const {
+        const uint64_t cnt = dcnt ? (*dcnt < this->cnt ? *dcnt : this->cnt) : this->cnt;
         uint64_t k = keys[i];
         const uint64_t gid = k >> KB;
         pl.val = vals[i];
@@ -318,9 +322,9 @@ struct RoundStore {
     }
 };
 
-static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, uint32_t *R, uint32_t *sa,
-                                uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1,
-                                uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s);
+static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, const uint32_t *d_cnt0,
+                                uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0,
+                                uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s);
 
 // One scan (L or S): resolves the chains of every item of the given type.
 template <class C, bool STYPE>
@@ -348,17 +352,31 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
     }
     uint32_t cnt = 0;
     PSK_TRY(ctx.read_u32(d_cnt, &cnt));
-    return doubling_rounds(ctx, n, nbuckets, cnt, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, STYPE ? 'S' : 'L', s);
+    return doubling_rounds(ctx, n, nbuckets, cnt, d_cnt, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, STYPE ? 'S' : 'L', s);
 }
 
+// Rounds of a work list shorter than this run DOUBLING_SPEC_ROUNDS at a
+// time without a host round trip between them: the counts stay on the
+// device (each kernel reads the current one and the launches are sized for
+// the count at the start of the block), the key width covers any group id
+// the block can meet, and every radix pass runs.  A round left with no
+// items costs a handful of empty launches, less than a read-back.
+constexpr uint32_t DOUBLING_SPEC_MAX = 1u << 20;
+constexpr int DOUBLING_SPEC_ROUNDS = 2;
+
 // Rank-doubling rounds over the work list (Wg = dense group id, Wv =
-// position) until every item has its own slot.
-static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, uint32_t *R, uint32_t *sa,
-                                uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1,
-                                uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s) {
+// position) until every item has its own slot.  `d_cnt0`: the device word
+// holding cnt (the work list's count).
+static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, const uint32_t *d_cnt0,
+                                uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0,
+                                uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s) {
     const int KB = bitlen(n);
     uint64_t ngroups = nbuckets;
-    Tri *d_tri = (Tri *)(ctx.d_scalars + 4);
+    // round totals alternate between two device slots: a round reads its
+    // count from the one the previous round wrote
+    Tri *d_tri[2] = {(Tri *)(ctx.d_scalars + 4), (Tri *)(ctx.d_scalars + 8)};
+    int tb = 0;
+    const uint32_t *dcnt = d_cnt0;
     // The work list (Wg, Wv) lives as two u32 arrays inside the key array of
     // the radix pair that is spare: it enters in (k1, v1), the keys are built
     // into the other pair, and each round writes the next list into whichever
@@ -367,37 +385,50 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
     uint32_t *vA = v0, *vB = v1;
     if (Wg != (uint32_t *)k1 || Wv != Wg + n)
         return set_error(PSACAK_EINTERNAL, "doubling rounds: work list outside its radix pair");
-    for (uint64_t h = 1; cnt > 0; h <<= 1) {
-        PSK_TRY(ctx.checkpoint());
-        const int GB = bitlen(ngroups > 0 ? ngroups - 1 : 0);
+    uint64_t h = 1;
+    while (cnt > 0) {
         if (h > n) return set_error(PSACAK_EINTERNAL, "doubling scan did not converge (n=%llu)", (unsigned long long)n);
-        uint64_t gblocks = ceil_div(cnt, 256 * 16);
-        PSK_CUDA(cudaMemsetAsync(ctx.d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
-        PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
-                        (k_keys<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
-                            Wg, Wv, cnt, R, n, h, KB, kA, vA, KB + GB, ctx.d_hist, ctx.d_err)));
-        PSK_LAUNCH_CHECK();
-        int in1 = 0;
-        PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(kA, vA, kB, vB, cnt, 0, KB + GB, &in1, true)));
-        uint64_t *ks = in1 ? kB : kA, *kfree = in1 ? kA : kB;
-        uint32_t *vs = in1 ? vB : vA, *vfree = in1 ? vA : vB;
-        Wg = (uint32_t *)kfree;
-        Wv = Wg + n;
-        PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, ngroups, KB, ctx.d_err},
-                                      RoundStore{gB, R, sa, Wg, Wv, n, ctx.d_err}, cnt, d_tri, OpTri(),
-                                      "scan_rounds")));
-        kA = ks;
-        vA = vs;
-        kB = kfree;
-        vB = vfree;
+        const bool spec = cnt < DOUBLING_SPEC_MAX;
+        const int rounds = spec ? DOUBLING_SPEC_ROUNDS : 1;
+        for (int r = 0; r < rounds && h <= n; r++) {
+            PSK_TRY(ctx.checkpoint());
+            // group ids: < ngroups in the block's first round, and later
+            // below the items left (kept subgroups never outnumber them)
+            const uint64_t gbound = r == 0 ? ngroups : (cnt > 0 ? cnt : 1);
+            const int GB = bitlen(gbound > 0 ? gbound - 1 : 0);
+            const uint32_t *dc = spec ? dcnt : nullptr;
+            uint64_t gblocks = ceil_div(cnt, 256 * 16);
+            PSK_CUDA(cudaMemsetAsync(ctx.d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
+            PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
+                            (k_keys<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
+                                Wg, Wv, cnt, dc, R, n, h, KB, kA, vA, KB + GB, ctx.d_hist, ctx.d_err)));
+            PSK_LAUNCH_CHECK();
+            int in1 = 0;
+            PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(kA, vA, kB, vB, cnt, 0, KB + GB, &in1, true, dc)));
+            uint64_t *ks = in1 ? kB : kA, *kfree = in1 ? kA : kB;
+            uint32_t *vs = in1 ? vB : vA, *vfree = in1 ? vA : vB;
+            Wg = (uint32_t *)kfree;
+            Wv = Wg + n;
+            Tri *tout = d_tri[tb];
+            PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, gbound, KB, ctx.d_err, dc},
+                                          RoundStore{gB, R, sa, Wg, Wv, n, ctx.d_err}, cnt, tout, OpTri(),
+                                          "scan_rounds", dc)));
+            kA = ks;
+            vA = vs;
+            kB = kfree;
+            vB = vfree;
+            dcnt = &tout->k;
+            tb ^= 1;
+            std::swap(gA, gB);
+            if (ctx.stage_timing)
+                fprintf(stderr, "[psacak]   doubling %c-scan h=%llu: <= %u items, %d key bits%s\n", tag,
+                        (unsigned long long)h, cnt, KB + GB, spec ? " (count on the device)" : "");
+            h <<= 1;
+        }
         uint32_t tri[4];
-        PSK_TRY(ctx.read_u32((const uint32_t *)d_tri, tri, 4));
-        if (ctx.stage_timing)
-            fprintf(stderr, "[psacak]   doubling %c-scan h=%llu: %u items, %d key bits -> %u unresolved in %llu groups\n",
-                    tag, (unsigned long long)h, cnt, KB + GB, tri[2], (unsigned long long)tri[3]);
+        PSK_TRY(ctx.read_u32(dcnt - 2, tri, 4));  // the last round's totals (g, s, k, o)
         cnt = tri[2];
         ngroups = tri[3];
-        std::swap(gA, gB);
     }
     return PSACAK_OK;
 }
@@ -459,7 +490,8 @@ status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bhead
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
     PSK_TRY(ctx.compact(AllPred{}, AllEmit{names, bheads, Wg, Wv, R}, n, ctx.d_scalars, "double_items"));
-    return doubling_rounds(ctx, n, nbuckets, (uint32_t)n, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, 'A', s);
+    return doubling_rounds(ctx, n, nbuckets, (uint32_t)n, ctx.d_scalars, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, 'A',
+                           s);
 }
 
 template status_t induce_doubling<uint8_t>(Ctx &, const uint8_t *, uint64_t, const uint32_t *, const uint32_t *,

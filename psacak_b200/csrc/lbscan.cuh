@@ -74,10 +74,13 @@ template <class T> __device__ __forceinline__ void set_word(T &v, int f, uint32_
     reinterpret_cast<uint32_t *>(&v)[f] = w;
 }
 
+// `dn` (nullable): the item count lives on the device (written by an earlier
+// kernel); the launch covers n_max items and the tiles past the count exit
+// at once (with no items at all, tile 0 writes the identity as the total).
 template <class T, class Op, class Load, class Store>
-__global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t n, Op op, uint64_t *flags,
-                                                     uint32_t *ticket, uint32_t epoch, uint32_t ntiles,
-                                                     T *total_out, uint32_t *err) {
+__global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t n_max, Op op, uint64_t *flags,
+                                                     uint32_t *ticket, uint32_t epoch, uint32_t ntiles_max,
+                                                     T *total_out, uint32_t *err, const uint32_t *dn) {
     constexpr int IPT = scan_ipt<T, Load>();
     constexpr int TILE = LS_BLOCK * IPT;
     constexpr int NF = Op::kFields;
@@ -90,6 +93,18 @@ __global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
+    uint64_t n = n_max;
+    uint32_t ntiles = ntiles_max;
+    if (dn) {
+        const uint64_t d = *dn;
+        if (d > n_max && tile == 0 && threadIdx.x == 0) dev_fail(err, DEVERR_RANGE);
+        n = d < n_max ? d : n_max;
+        ntiles = (uint32_t)((n + TILE - 1) / TILE);
+        if (tile >= ntiles) {
+            if (tile == 0 && threadIdx.x == 0 && total_out) *total_out = Op::identity();
+            return;
+        }
+    }
     const uint64_t base = (uint64_t)tile * TILE;
     T v[IPT];
     typename PL::type pl[IPT];
@@ -170,9 +185,10 @@ __global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t
 
 // Runs the scan; `total_out` (device, nullable) receives the aggregate of
 // all items (the identity when n == 0).
+// `dn` (nullable): the item count is read on the device (at most n).
 template <class T, class Op, class Load, class Store>
 status_t lb_scan(Load ld, Store st, uint64_t n, T *total_out, Op op, ScanScratch &ss, OnesweepScratch &os,
-                 uint32_t *err, cudaStream_t s, const char *pname = "scan") {
+                 uint32_t *err, cudaStream_t s, const char *pname = "scan", const uint32_t *dn = nullptr) {
     if (n == 0) {
         if (total_out) PSK_CUDA(cudaMemsetAsync(total_out, 0, sizeof(T), s));
         return PSACAK_OK;
@@ -186,7 +202,7 @@ status_t lb_scan(Load ld, Store st, uint64_t n, T *total_out, Op op, ScanScratch
     PSK_CUDA(cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s));
     PSK_PROF_LAUNCH(s, pname, n, 0,
                     (k_lbscan<T, Op, Load, Store><<<(uint32_t)ntiles, LS_BLOCK, 0, s>>>(
-                        ld, st, n, op, ss.flags, ticket, os.epoch, (uint32_t)ntiles, total_out, err)));
+                        ld, st, n, op, ss.flags, ticket, os.epoch, (uint32_t)ntiles, total_out, err, dn)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }

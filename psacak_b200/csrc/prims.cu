@@ -9,6 +9,7 @@
 namespace psk {
 
 std::atomic<uint64_t> g_kernel_launches{0};
+std::atomic<uint64_t> g_round_trips{0};
 thread_local Profiler *t_prof = nullptr;
 
 static thread_local char t_last_error[512] = "";
@@ -37,6 +38,7 @@ __global__ void k_copy_words(const uint32_t *__restrict__ src, uint32_t *dst, ui
 
 status_t read_back(const uint32_t *d, uint32_t *mapped, uint32_t count, cudaStream_t s) {
     if (count == 0) return PSACAK_OK;
+    PSK_ROUND_TRIP();
     k_copy_words<<<1, 256, 0, s>>>(d, mapped, count);
     PSK_KCOUNT();
     PSK_CUDA(cudaGetLastError());

@@ -12,6 +12,10 @@ namespace psk {
 
 extern std::atomic<uint64_t> g_kernel_launches;
 #define PSK_KCOUNT() (::psk::g_kernel_launches.fetch_add(1, std::memory_order_relaxed))
+// Host round trips inside a build: the host waits for values the device
+// computed (counts, histograms) before it can decide what to launch next.
+extern std::atomic<uint64_t> g_round_trips;
+#define PSK_ROUND_TRIP() (::psk::g_round_trips.fetch_add(1, std::memory_order_relaxed))
 }  // namespace psk
 #include "prof.cuh"
 namespace psk {

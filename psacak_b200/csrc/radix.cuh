@@ -1,8 +1,10 @@
 // radix.cuh -- LSD radix sort of (key, value) pairs on 8-bit digits.
 //
 // One histogram kernel reads the keys once and counts the digits of every
-// pass; the host reads those counts (one sync per sort) and skips passes in
-// which a single digit holds every key.  Each remaining pass is one
+// pass; for sorts of RADIX_PROBE_MIN keys or more the host reads those
+// counts (one sync per sort) and skips passes in which a single digit holds
+// every key.  Shorter sorts run every pass without that round trip (a pass
+// over fewer keys costs less than the read-back).  Each pass is one
 // onesweep kernel (single-pass stable scatter with decoupled look-back).
 #pragma once
 
@@ -12,6 +14,7 @@
 namespace psk {
 
 constexpr int RADIX_MAX_PASSES = 8;
+constexpr uint64_t RADIX_PROBE_MIN = 1ull << 20;
 constexpr int RADIX_HIST_BLOCK = 256;
 
 // One radix pass as a TMA-fed onesweep tile.  A full tile's keys and values
@@ -65,11 +68,13 @@ __device__ __forceinline__ void radix_rank(const K *s_k, uint32_t cnt, int shift
 constexpr int RS_MIN_BLOCKS = 4;
 constexpr int RADIX_IPT = 12;  // items per thread of the radix passes (3072-item tiles)
 
+// `dn` (nullable): the key count is read on the device (at most n_max, the
+// count the grid was sized for); tiles past it exit at once.
 template <class K, class V, int IPT>
 __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
     k_radix_pass(const K *__restrict__ kin, const V *__restrict__ vin, K *__restrict__ kout, V *__restrict__ vout,
-                 int shift, uint32_t dmask, const uint32_t *__restrict__ dbase, uint64_t n, int bulk_ok,
-                 uint64_t *status, uint32_t *ticket, uint32_t epoch, uint32_t *err) {
+                 int shift, uint32_t dmask, const uint32_t *__restrict__ dbase, uint64_t n_max, int bulk_ok,
+                 uint64_t *status, uint32_t *ticket, uint32_t epoch, uint32_t *err, const uint32_t *dn) {
     constexpr int TILE = OS_BLOCK * IPT;
     extern __shared__ __align__(128) unsigned char rs_smem[];
     K *s_k = (K *)rs_smem;
@@ -93,6 +98,12 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint64_t base = (uint64_t)tile * TILE;
+    uint64_t n = n_max;
+    if (dn) {
+        const uint64_t d = *dn;
+        n = d < n_max ? d : n_max;
+        if (base >= n) return;  // the whole CTA: no copy was issued
+    }
     const uint32_t cnt = (uint32_t)(n - base < (uint64_t)TILE ? n - base : (uint64_t)TILE);
     const bool bulk = bulk_ok && cnt == (uint32_t)TILE;
     if (bulk) {
@@ -158,7 +169,7 @@ __global__ void __launch_bounds__(OS_BLOCK, RS_MIN_BLOCKS)
 
 template <class K, class V, int IPT>
 status_t radix_pass(const K *kin, const V *vin, K *kout, V *vout, int shift, uint32_t dmask, const uint32_t *dbase,
-                    uint64_t n, OnesweepScratch &sc, uint32_t *err, cudaStream_t s) {
+                    uint64_t n, OnesweepScratch &sc, uint32_t *err, cudaStream_t s, const uint32_t *dn = nullptr) {
     constexpr int TILE = OS_BLOCK * IPT;
     const uint64_t ntiles = ceil_div(n, TILE);
     if (ntiles > sc.max_tiles) return set_error(PSACAK_EINTERNAL, "radix pass: %llu tiles exceed scratch", (unsigned long long)ntiles);
@@ -172,7 +183,7 @@ status_t radix_pass(const K *kin, const V *vin, K *kout, V *vout, int shift, uin
     PSK_CUDA(cudaFuncSetAttribute(k_radix_pass<K, V, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     PSK_PROF_LAUNCH(s, "radix_pass", n, 2 * n * (sizeof(K) + sizeof(V)),
                     (k_radix_pass<K, V, IPT><<<(uint32_t)ntiles, OS_BLOCK, smem, s>>>(
-                        kin, vin, kout, vout, shift, dmask, dbase, n, bulk_ok, sc.status, ticket, sc.epoch, err)));
+                        kin, vin, kout, vout, shift, dmask, dbase, n, bulk_ok, sc.status, ticket, sc.epoch, err, dn)));
     PSK_LAUNCH_CHECK();
     return PSACAK_OK;
 }
@@ -249,11 +260,12 @@ status_t read_back(const uint32_t *d, uint32_t *mapped, uint32_t count, cudaStre
 
 // When `hist_ready` is set, the producer of the keys has already counted
 // the digits of every pass into d_hist (see radix_count_digits), and the
-// histogram kernel is skipped.
+// histogram kernel is skipped.  `dn` (nullable): the key count is on the
+// device, n is its bound; every pass runs (nothing to probe on the host).
 template <class K, class V>
 status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit, int end_bit, uint32_t *d_hist,
                           uint32_t *h_hist, uint32_t *h_hist_mapped, OnesweepScratch &sc, uint32_t *err, int *result_in_1, cudaStream_t s,
-                          int ipt = 12, bool hist_ready = false) {
+                          int ipt = 12, bool hist_ready = false, const uint32_t *dn = nullptr) {
     *result_in_1 = 0;
     if (n <= 1 || end_bit <= begin_bit) return PSACAK_OK;
     const int npasses = (end_bit - begin_bit + 7) / 8;
@@ -267,24 +279,27 @@ status_t radix_sort_pairs(K *k0, V *v0, K *k1, V *v1, uint64_t n, int begin_bit,
                             k0, n, begin_bit, npasses, end_bit, d_hist)));
     }
     PSK_PROF_LAUNCH(s, "radix_bases", npasses * 256, 0, (k_radix_bases<<<npasses, 256, 0, s>>>(d_hist, bases)));
-    PSK_TRY(read_back(d_hist, h_hist_mapped, npasses * 256, s));
+    if (dn && !hist_ready) return set_error(PSACAK_EINTERNAL, "radix sort: a device count needs counted digits");
+    const bool probe = !dn && n >= RADIX_PROBE_MIN;
+    if (probe) PSK_TRY(read_back(d_hist, h_hist_mapped, npasses * 256, s));
     K *ki = k0, *ko = k1;
     V *vi = v0, *vo = v1;
     int flip = 0;
     for (int p = 0; p < npasses; p++) {
         bool trivial = false;
-        for (int d = 0; d < 256; d++)
-            if (h_hist[p * 256 + d] == n) trivial = true;
+        if (probe)
+            for (int d = 0; d < 256; d++)
+                if (h_hist[p * 256 + d] == n) trivial = true;
         if (trivial) continue;
         int shift = begin_bit + 8 * p;
         int bits = end_bit - shift < 8 ? end_bit - shift : 8;
         const uint32_t dmask = (1u << bits) - 1;
         if (ipt == 8) {
-            PSK_TRY((radix_pass<K, V, 8>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s)));
+            PSK_TRY((radix_pass<K, V, 8>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s, dn)));
         } else if (ipt == 16) {
-            PSK_TRY((radix_pass<K, V, 16>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s)));
+            PSK_TRY((radix_pass<K, V, 16>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s, dn)));
         } else {
-            PSK_TRY((radix_pass<K, V, 12>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s)));
+            PSK_TRY((radix_pass<K, V, 12>(ki, vi, ko, vo, shift, dmask, bases + p * 256, n, sc, err, s, dn)));
         }
         K *tk = ki; ki = ko; ko = tk;
         V *tv = vi; vi = vo; vo = tv;
