@@ -652,8 +652,8 @@ def measure_batch(args, torch, ctx, dev, dist, world, rank, texts, steps, warmup
         ctx.psacak8_batch_dev(d_texts.data_ptr(), off, d_sas.data_ptr(), stream.cuda_stream, sc)
 
     # the library's NULL schedule, spelled out (the autotuner's start point)
-    default = {"engine": 1, "tile_items": 8, "scan_ctas_per_sm": 4, "batch_chunk_mib": 3072,
-               "finish_below": 1 << 16}
+    default = {"engine": 1, "tile_items": 16, "scan_ctas_per_sm": 4, "batch_chunk_mib": 3072,
+               "finish_below": 1 << 26}
     if base_sched:
         default.update(base_sched)
     tuned = None

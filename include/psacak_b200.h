@@ -42,9 +42,13 @@ extern "C" {
 
 /* Tunables of one build.  Zero fields mean "use the default" (finish_below:
  * 0 = never).  A NULL schedule is the zero schedule with finish_below =
- * PSACAK_DEFAULT_FINISH_BELOW.  Every schedule gives the same suffix array;
- * it only changes speed. */
-#define PSACAK_DEFAULT_FINISH_BELOW (1u << 16)
+ * PSACAK_DEFAULT_FINISH_BELOW and tile_items = PSACAK_DEFAULT_TILE_ITEMS:
+ * the single schedule with the smallest total time on the texts the
+ * schedule selector was trained on (lengths 4 KiB..64 MiB), and the fastest
+ * one for a 1 GiB genome-like text too.  Every schedule gives the same
+ * suffix array; it only changes speed. */
+#define PSACAK_DEFAULT_FINISH_BELOW (1u << 26)
+#define PSACAK_DEFAULT_TILE_ITEMS 16u
 typedef struct {
     uint32_t engine;           /* PSACAK_ENGINE_* for level 0 */
     uint32_t inner_engine;     /* PSACAK_ENGINE_* for levels >= 1 */

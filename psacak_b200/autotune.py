@@ -23,7 +23,7 @@ batched build uses to pick chunk size and block shape.
 import math
 
 BATCH_SPACE = {
-    "finish_below": [0, 1 << 13, 1 << 16, 1 << 20],
+    "finish_below": [0, 1 << 13, 1 << 16, 1 << 20, 1 << 22, 1 << 26],
     "batch_chunk_mib": [256, 512, 1024, 3072],
     "tile_items": [8, 12, 16],
     "scan_ctas_per_sm": [2, 4, 8],

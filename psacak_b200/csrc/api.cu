@@ -627,7 +627,12 @@ void ctx_free(Ctx &c) {
 static void apply_schedule(Ctx &c, const psacak_schedule *sched) {
     psacak_schedule d{};
     if (sched) d = *sched;
-    else d.finish_below = PSACAK_DEFAULT_FINISH_BELOW;  // short texts: prefix doubling (far fewer round trips)
+    else {
+        // levels under 64 Mi symbols by prefix doubling (fewer round trips
+        // than recursion), 16-item tiles
+        d.finish_below = PSACAK_DEFAULT_FINISH_BELOW;
+        d.tile_items = PSACAK_DEFAULT_TILE_ITEMS;
+    }
     c.sched = d;
     uint32_t per = d.scan_ctas_per_sm ? d.scan_ctas_per_sm : 4;
     c.scan_ctas = per * (uint32_t)c.dev.num_sms;

@@ -36,8 +36,8 @@ SCHEDULES = [
     for t in (8, 16) for f in FINISH_GRID
 ]
 # The schedule a NULL psacak_schedule stands for (include/psacak_b200.h).
-LIBRARY_DEFAULT = {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 8,
-                   "finish_below": 1 << 16}
+LIBRARY_DEFAULT = {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 16,
+                   "finish_below": 1 << 26}
 DEFAULT_INDEX = SCHEDULES.index(LIBRARY_DEFAULT)
 
 

@@ -48,6 +48,22 @@ def _u32(t):
     return t.cpu().numpy().view(np.uint32)
 
 
+DEFAULT_FINISH_BELOW = 1 << 26  # PSACAK_DEFAULT_FINISH_BELOW
+
+
+def _levels_match(got, want, finish_below):
+    """The levels a build recursed through are the oracle's; from the first
+    level shorter than finish_below on, the build sorted directly by prefix
+    doubling (one record, no LMS count) where the oracle recursed further."""
+    assert len(got) <= len(want)
+    for i, (lv, w) in enumerate(zip(got, want)):
+        if finish_below and lv["m"] < finish_below and w["n_lms"] > 0:
+            assert lv["m"] == w["m"] and lv["n_lms"] == 0 and i == len(got) - 1
+            return
+        assert lv == w
+    assert len(got) == len(want)
+
+
 def test_genome_1gib_matches_oracle(ctx):
     fx = load("fullsize_genome1g.json")
     n = fx["n"]
@@ -57,9 +73,15 @@ def test_genome_1gib_matches_oracle(ctx):
     ds = torch.empty(n, dtype=torch.int32, device="cuda")
     ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream, None)
     torch.cuda.synchronize()
-    assert ctx.trace() == fx["levels"]
+    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH_BELOW)
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     assert ctx.check_sa8_dev(dt.data_ptr(), n, ds.data_ptr(), stream)
+    # the zero schedule recurses all the way down, as the oracle does
+    ds.zero_()
+    ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {"engine": pk.ENGINE_BUCKET})
+    torch.cuda.synchronize()
+    assert ctx.trace() == fx["levels"]
+    assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     del ds, dt
     torch.cuda.empty_cache()
     # host pointers, pageable output: the drop-in for psacak_inplace
@@ -79,15 +101,7 @@ def test_zipf32_256m_matches_oracle(ctx):
     torch.cuda.synchronize()
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     # the levels the default schedule recursed through are the oracle's
-    got = ctx.trace()
-    assert len(got) <= len(fx["levels"])
-    for lv, want in zip(got, fx["levels"]):
-        if lv["n_lms"] == 0 and want["n_lms"] > 0:
-            # the library's default finish_below (2^16): sorted directly by
-            # prefix doubling from this level on
-            assert lv["m"] == want["m"] and lv["m"] < (1 << 16)
-            break
-        assert lv == want
+    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH_BELOW)
     ds.zero_()
     ctx.psacak32_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {})  # zero schedule: no finisher
     torch.cuda.synchronize()

@@ -82,15 +82,16 @@ def test_selector_beats_the_best_fixed_schedule(ctx):
     rng = np.random.default_rng(5)
 
     def texts(count, seed):
+        # both kinds at 3..8 MiB, so that no length cut-off separates them
         out = []
         for i in range(count):
-            n = int(np.exp(rng.uniform(np.log(1 << 20), np.log(6 << 20))))
+            n = int(np.exp(rng.uniform(np.log(3 << 20), np.log(8 << 20))))
             if i % 2 == 0:
                 out.append((synth.iid(n, b"ACGT", seed=seed + i), 1))
             else:
-                block = synth.iid(int(rng.integers(2000, 9000)), b"ACGT", seed=seed + i)
+                block = synth.iid(int(rng.integers(500, 2000)), b"ACGT", seed=seed + i)
                 t = np.resize(block, n)
-                t[rng.integers(0, n, 8)] = ord("N")  # a few mutations, so the repeats are not exact to the end
+                t[rng.integers(0, n, 3)] = ord("N")  # a few mutations: repeats of about n/4 symbols
                 out.append((t, 1))
         return out
 
@@ -115,6 +116,9 @@ def test_selector_beats_the_best_fixed_schedule(ctx):
     best_ms = Tte.min(axis=1).sum()
     print("held-out: per-text best %.2f ms, selector %.2f ms, best fixed (%s) %.2f ms"
           % (best_ms, sel_ms, sel.SCHEDULES[best_fixed], fixed_ms))
+    for i in range(len(Tte)):
+        print("  text %d: best %.2f (#%d), pick %.2f (#%d), fixed %.2f" % (
+            i, Tte[i].min(), int(Tte[i].argmin()), Tte[i, picks[i]], picks[i], Tte[i, best_fixed]))
     assert sel_ms <= 0.9 * fixed_ms
     # every picked schedule builds the oracle's suffix array
     for t, w in texts(4, 7000):
