@@ -357,7 +357,9 @@ def run_b200(args):
     n = text.size
     ctx = pk.Context(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if args.workload == "iid8m" else None
-    sched = {"engine": args.engine}
+    # the plain form is the library's default schedule (a NULL schedule);
+    # --engine picks a level-0 engine with every other field zero instead
+    sched = None if args.engine == 0 else {"engine": args.engine}
     d_text = torch.from_numpy(text).to(dev)
     d_sa = torch.empty(n, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -442,6 +444,30 @@ def run_b200(args):
     build_bytes = algorithmic_build_bytes(trace)
     build_gbs = build_bytes / (ms / 1000.0) / 1e9
 
+    def timed_steps(sc):
+        """Device ms per build with schedule sc, timed as the plain form
+        (warm-up builds first; L2 flushed between steps for small inputs)."""
+        for _ in range(max(1, args.warmup)):
+            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, sc)
+        torch.cuda.synchronize(dev)
+        total = 0.0
+        if flush is None:
+            e0.record(stream)
+            for _ in range(args.steps):
+                ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, sc)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            total = e0.elapsed_time(e1)
+        else:
+            for _ in range(args.steps):
+                flush.fill_(1)
+                e0.record(stream)
+                ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, sc)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                total += e0.elapsed_time(e1)
+        return _max_over_ranks(torch, dist, dev, total / args.steps)
+
     # learned-schedule form: the selector picks a schedule from the text's
     # statistics (inference kernel), timed the same way as the plain form
     learned = None
@@ -454,18 +480,23 @@ def run_b200(args):
         feats = sel.features(ctx, d_text.data_ptr(), n, 1)
         choice, _ = net.predict(feats)
         lsched = dict(sel.SCHEDULES[choice])
-        for _ in range(max(1, args.warmup)):
-            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, lsched)
-        torch.cuda.synchronize(dev)
-        e0.record(stream)
-        for _ in range(args.steps):
-            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, lsched)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        lms_ = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+        lms_ = timed_steps(lsched)
         lok = None if args.no_verify else ctx.check_sa8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream)
         learned = {"value": world * n / (lms_ / 1000.0), "unit": UNIT, "ms_per_step": lms_, "schedule": lsched,
                    "verified": lok, "hbm_gbs_algorithmic_build": build_bytes / (lms_ / 1000.0) / 1e9}
+    # zero schedule: every field 0, SACA-K with recursion down to the last
+    # level as the reference does (the default sorts short levels directly)
+    zero = None
+    if not args.single_build:
+        zs = {"engine": 0}
+        zr0 = ctx.round_trips()
+        zms = timed_steps(zs)
+        zrt = (ctx.round_trips() - zr0) // (max(1, args.warmup) + args.steps)
+        zok = None if args.no_verify else ctx.check_sa8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream)
+        zero = {"value": world * n / (zms / 1000.0), "unit": UNIT, "ms_per_step": zms, "schedule": zs,
+                "host_round_trips_per_step": zrt, "verified": zok,
+                "note": "every field 0: induced sorting and recursion on every level, as the reference"}
+
     # autotuned form: exhaustive search over the selector's schedules on
     # this text (the selector's fallback and yardstick), timed as above
     autotuned = None
@@ -477,15 +508,7 @@ def run_b200(args):
         best_i, table = autotune.exhaustive(tf, sel.SCHEDULES)
         tune_s = time.perf_counter() - t0
         asched = dict(sel.SCHEDULES[best_i])
-        for _ in range(max(1, args.warmup)):
-            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, asched)
-        torch.cuda.synchronize(dev)
-        e0.record(stream)
-        for _ in range(args.steps):
-            ctx.psacak8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, asched)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        ams = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+        ams = timed_steps(asched)
         aok = None if args.no_verify else ctx.check_sa8_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream)
         autotuned = {"value": world * n / (ams / 1000.0), "unit": UNIT, "ms_per_step": ams, "schedule": asched,
                      "verified": aok, "search": "exhaustive over %d schedules (min of 1 build each, after a "
@@ -573,7 +596,9 @@ def run_b200(args):
             "e2e": e2e, "e2e_pinned": e2e_pinned, "roofline": roofline, "learned_schedule": learned,
             "autotuned_schedule": autotuned,
             "batched": batched,
-            "plain_schedule": {"engine": args.engine, "note": "library default schedule (the value above)"},
+            "plain_schedule": {"schedule": sched if sched is not None else "NULL (library default)",
+                               "note": "the value above"},
+            "zero_schedule": zero,
             "hbm_gbs_algorithmic_build": build_gbs,
             "build_algorithmic_bytes": build_bytes,
             "cpu_baseline": cpu, "cpu_baseline_all_cores": cpu_all, "clocks": clk, "gpu_launches": int(launches),

@@ -41,8 +41,10 @@ __global__ void k_phi(const uint32_t *__restrict__ sa, uint64_t n, uint32_t *phi
 // Symbols one thread compares for an irreducible position before handing
 // it to a whole CTA (k_plcp_long): a long run of one character has a single
 // irreducible position whose PLCP is about the run's length, which one
-// thread would walk alone.
-constexpr uint32_t LCP_THREAD_MAX = 1024;
+// thread would walk alone.  Set high enough that the many irreducible
+// positions of moderately long repeats (a genome's copies) stay with their
+// threads, which run side by side.
+constexpr uint32_t LCP_THREAD_MAX = 16384;
 constexpr int LCP_LONG_BLOCK = 256;
 constexpr int LCP_LONG_SYMS = 16;  // per thread and step: 4096 symbols per CTA step
 

@@ -73,7 +73,7 @@ def test_lcp_run_heavy_texts_finish_quickly(ctx):
     texts = [np.concatenate([np.full(8 << 20, 65, np.uint8), rng.integers(65, 69, 1000).astype(np.uint8)]),
              np.concatenate([rng.integers(65, 69, 5000).astype(np.uint8), np.full(3_000_017, 67, np.uint8),
                              np.tile(np.frombuffer(b"ACGTTGCA", np.uint8), 200_000),
-                             np.full(1023, 71, np.uint8), np.full(1025, 84, np.uint8)]),
+                             np.full(16383, 71, np.uint8), np.full(16385, 84, np.uint8)]),
              np.tile(synth.iid(5000, b"ACGT", seed=3), 300)]
     for t in texts:
         n = t.size
