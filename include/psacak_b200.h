@@ -41,13 +41,18 @@ extern "C" {
 #define PSACAK_ENGINE_DOUBLING 2 /* chain-doubling scan (any alphabet) */
 
 /* Tunables of one build.  Zero fields mean "use the default" (finish_below:
- * 0 = never).  A NULL schedule is the zero schedule with finish_below =
- * PSACAK_DEFAULT_FINISH_BELOW and tile_items = PSACAK_DEFAULT_TILE_ITEMS:
- * the single schedule with the smallest total time on the texts the
- * schedule selector was trained on (lengths 4 KiB..64 MiB), and the fastest
- * one for a 1 GiB genome-like text too.  Every schedule gives the same
- * suffix array; it only changes speed. */
+ * 0 = never; inner_finish_below: 0 = finish_below).  A NULL schedule is the
+ * zero schedule with finish_below = PSACAK_DEFAULT_FINISH_BELOW,
+ * inner_finish_below = PSACAK_DEFAULT_INNER_FINISH_BELOW and tile_items =
+ * PSACAK_DEFAULT_TILE_ITEMS: texts under 64 Mi symbols sorted directly by
+ * prefix doubling (the single schedule with the smallest total time on the
+ * texts the schedule selector was trained on, 4 KiB..64 MiB), longer texts
+ * by induced sorting at the top level and prefix doubling from the first
+ * reduced string on (the fastest schedule measured for a 1 GiB genome-like
+ * text).  Every schedule gives the same suffix array; it only changes
+ * speed. */
 #define PSACAK_DEFAULT_FINISH_BELOW (1u << 26)
+#define PSACAK_DEFAULT_INNER_FINISH_BELOW (1u << 30)
 #define PSACAK_DEFAULT_TILE_ITEMS 16u
 typedef struct {
     uint32_t engine;           /* PSACAK_ENGINE_* for level 0 */
@@ -58,7 +63,9 @@ typedef struct {
     uint32_t finish_below;     /* recursion strategy: levels shorter than this (the text itself
                                   included) are sorted directly by prefix doubling instead of
                                   induced sorting and recursion (0 = never) */
-    uint32_t reserved[2];
+    uint32_t inner_finish_below; /* the same cut-off for the reduced strings (levels >= 1),
+                                    0 = finish_below */
+    uint32_t reserved[1];
 } psacak_schedule;
 
 /* One record per recursion level of the last build on a context. */

@@ -62,7 +62,8 @@ class Schedule(ctypes.Structure):
         ("batch_chunk_mib", ctypes.c_uint32),
         ("tile_items", ctypes.c_uint32),
         ("finish_below", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 2),
+        ("inner_finish_below", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 1),
     ]
 
 

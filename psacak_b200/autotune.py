@@ -11,7 +11,8 @@ Every schedule builds the same suffix array; the knobs only change speed:
 * ``batch_chunk_mib``   largest concatenated build of a batch (the chunk size);
 * ``finish_below``      recursion strategy: levels shorter than this are
                         sorted directly by prefix doubling; in a batch, texts
-                        of at most 8 KiB below it go to one CTA each.
+                        of at most 8 KiB below it go to one CTA each;
+* ``inner_finish_below`` the same cut-off for the reduced strings.
 
 ``exhaustive`` times a list of schedules (the fallback of the learned
 selector and the yardstick of its regret).  ``coordinate_descent`` searches
@@ -28,8 +29,9 @@ BATCH_SPACE = {
     "tile_items": [8, 12, 16],
     "scan_ctas_per_sm": [2, 4, 8],
     "engine": [1, 2],
+    "inner_finish_below": [1 << 30, 1 << 26, 1 << 22],
 }
-BATCH_ORDER = ["finish_below", "batch_chunk_mib", "tile_items", "scan_ctas_per_sm", "engine"]
+BATCH_ORDER = ["finish_below", "inner_finish_below", "batch_chunk_mib", "tile_items", "scan_ctas_per_sm", "engine"]
 
 
 def device_timer(build, reps=1):

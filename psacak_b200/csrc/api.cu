@@ -169,8 +169,11 @@ status_t build_level(Ctx &ctx, const C *text, const uint32_t *names, const uint3
     }
     const bool bytes = sizeof(C) == 1;
     if constexpr (sizeof(C) == 4) {
-        // recursion finisher: short inner strings are sorted by prefix doubling
-        if (names && bheads && ctx.sched.finish_below && n < ctx.sched.finish_below) {
+        // recursion finisher: short strings are sorted by prefix doubling
+        // (the input's own cut-off at level 0, the inner one below it)
+        const uint32_t finish = level > 0 && ctx.sched.inner_finish_below ? ctx.sched.inner_finish_below
+                                                                          : ctx.sched.finish_below;
+        if (names && bheads && finish && n < finish) {
             trace_push(ctx, level, width, n, 0, 0, 0);
             if (n <= SMALL_MAX && nbuckets <= 65535)  // in one CTA's shared memory
                 return small_sa<uint32_t>(ctx, names, SmallJobs{nullptr, nullptr, 1, n, n}, (uint32_t)nbuckets, sa, s);
@@ -628,9 +631,10 @@ static void apply_schedule(Ctx &c, const psacak_schedule *sched) {
     psacak_schedule d{};
     if (sched) d = *sched;
     else {
-        // levels under 64 Mi symbols by prefix doubling (fewer round trips
-        // than recursion), 16-item tiles
+        // texts under 64 Mi symbols and reduced strings under 1 Gi symbols
+        // by prefix doubling (fewer round trips than recursion), 16-item tiles
         d.finish_below = PSACAK_DEFAULT_FINISH_BELOW;
+        d.inner_finish_below = PSACAK_DEFAULT_INNER_FINISH_BELOW;
         d.tile_items = PSACAK_DEFAULT_TILE_ITEMS;
     }
     c.sched = d;

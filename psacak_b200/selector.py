@@ -31,13 +31,17 @@ NH = 64
 # text is sorted by prefix doubling.
 ALWAYS = 0xFFFFFFFF
 FINISH_GRID = [0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, 1 << 24, 1 << 26, ALWAYS]
+# The reduced strings of every schedule use the library's inner cut-off
+# (1 Gi symbols): prefix doubling from the first reduced string on.
+INNER_FINISH = 1 << 30
 SCHEDULES = [
-    {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": t, "finish_below": f}
+    {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": t, "finish_below": f,
+     "inner_finish_below": INNER_FINISH}
     for t in (8, 16) for f in FINISH_GRID
 ]
 # The schedule a NULL psacak_schedule stands for (include/psacak_b200.h).
 LIBRARY_DEFAULT = {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 16,
-                   "finish_below": 1 << 26}
+                   "finish_below": 1 << 26, "inner_finish_below": INNER_FINISH}
 DEFAULT_INDEX = SCHEDULES.index(LIBRARY_DEFAULT)
 
 

@@ -48,16 +48,18 @@ def _u32(t):
     return t.cpu().numpy().view(np.uint32)
 
 
-DEFAULT_FINISH_BELOW = 1 << 26  # PSACAK_DEFAULT_FINISH_BELOW
+DEFAULT_FINISH = (1 << 26, 1 << 30)  # PSACAK_DEFAULT_FINISH_BELOW, PSACAK_DEFAULT_INNER_FINISH_BELOW
 
 
-def _levels_match(got, want, finish_below):
+def _levels_match(got, want, finish):
     """The levels a build recursed through are the oracle's; from the first
-    level shorter than finish_below on, the build sorted directly by prefix
-    doubling (one record, no LMS count) where the oracle recursed further."""
+    level shorter than its cut-off on (finish[0] for the input, finish[1]
+    for the reduced strings), the build sorted directly by prefix doubling
+    (one record, no LMS count) where the oracle recursed further."""
     assert len(got) <= len(want)
     for i, (lv, w) in enumerate(zip(got, want)):
-        if finish_below and lv["m"] < finish_below and w["n_lms"] > 0:
+        cut = finish[0] if i == 0 else finish[1]
+        if cut and lv["m"] < cut and w["n_lms"] > 0:
             assert lv["m"] == w["m"] and lv["n_lms"] == 0 and i == len(got) - 1
             return
         assert lv == w
@@ -73,9 +75,16 @@ def test_genome_1gib_matches_oracle(ctx):
     ds = torch.empty(n, dtype=torch.int32, device="cuda")
     ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream, None)
     torch.cuda.synchronize()
-    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH_BELOW)
+    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH)
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     assert ctx.check_sa8_dev(dt.data_ptr(), n, ds.data_ptr(), stream)
+    # induced sorting down to 64 Mi symbols, the old default's shape
+    ds.zero_()
+    ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {"engine": 1, "tile_items": 16,
+                                                             "finish_below": 1 << 26})
+    torch.cuda.synchronize()
+    _levels_match(ctx.trace(), fx["levels"], (1 << 26, 1 << 26))
+    assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     # the zero schedule recurses all the way down, as the oracle does
     ds.zero_()
     ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {"engine": pk.ENGINE_BUCKET})
@@ -101,7 +110,7 @@ def test_zipf32_256m_matches_oracle(ctx):
     torch.cuda.synchronize()
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     # the levels the default schedule recursed through are the oracle's
-    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH_BELOW)
+    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH)
     ds.zero_()
     ctx.psacak32_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {})  # zero schedule: no finisher
     torch.cuda.synchronize()
