@@ -678,7 +678,7 @@ def measure_batch(args, torch, ctx, dev, dist, world, rank, texts, steps, warmup
 
     # the library's NULL schedule, spelled out (the autotuner's start point)
     default = {"engine": 1, "tile_items": 16, "scan_ctas_per_sm": 4, "batch_chunk_mib": 3072,
-               "finish_below": 1 << 26, "inner_finish_below": 1 << 30}
+               "finish_below": 1 << 24, "inner_finish_below": 1 << 30}
     if base_sched:
         default.update(base_sched)
     tuned = None

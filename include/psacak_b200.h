@@ -42,16 +42,19 @@ extern "C" {
 
 /* Tunables of one build.  Zero fields mean "use the default" (finish_below:
  * 0 = never; inner_finish_below: 0 = finish_below).  A NULL schedule is the
- * zero schedule with finish_below = PSACAK_DEFAULT_FINISH_BELOW,
+ * zero schedule with finish_below = PSACAK_DEFAULT_FINISH_BELOW for byte
+ * texts and PSACAK_DEFAULT_FINISH_BELOW32 for integer texts,
  * inner_finish_below = PSACAK_DEFAULT_INNER_FINISH_BELOW and tile_items =
- * PSACAK_DEFAULT_TILE_ITEMS: texts under 64 Mi symbols sorted directly by
- * prefix doubling (the single schedule with the smallest total time on the
- * texts the schedule selector was trained on, 4 KiB..64 MiB), longer texts
- * by induced sorting at the top level and prefix doubling from the first
- * reduced string on (the fastest schedule measured for a 1 GiB genome-like
- * text).  Every schedule gives the same suffix array; it only changes
- * speed. */
-#define PSACAK_DEFAULT_FINISH_BELOW (1u << 26)
+ * PSACAK_DEFAULT_TILE_ITEMS: shorter texts are sorted directly by prefix
+ * doubling, longer ones by induced sorting at the top level and prefix
+ * doubling from the first reduced string on.  The cut-offs are the ones
+ * with the smallest total time on the texts the schedule selector was
+ * trained on (4 KiB..64 MiB; large byte texts sort faster by induced
+ * sorting, large integer texts by prefix doubling), and the inner one the
+ * fastest measured for a 1 GiB genome-like text.  Every schedule gives the
+ * same suffix array; it only changes speed. */
+#define PSACAK_DEFAULT_FINISH_BELOW (1u << 24)
+#define PSACAK_DEFAULT_FINISH_BELOW32 (1u << 26)
 #define PSACAK_DEFAULT_INNER_FINISH_BELOW (1u << 30)
 #define PSACAK_DEFAULT_TILE_ITEMS 16u
 typedef struct {

@@ -627,13 +627,15 @@ void ctx_free(Ctx &c) {
     c.h_pinned = nullptr;
 }
 
-static void apply_schedule(Ctx &c, const psacak_schedule *sched) {
+// `width`: symbol width of the input (1 = bytes, 4 = integer symbols), which
+// picks the default cut-off of a NULL schedule.
+static void apply_schedule(Ctx &c, const psacak_schedule *sched, int width) {
     psacak_schedule d{};
     if (sched) d = *sched;
     else {
-        // texts under 64 Mi symbols and reduced strings under 1 Gi symbols
-        // by prefix doubling (fewer round trips than recursion), 16-item tiles
-        d.finish_below = PSACAK_DEFAULT_FINISH_BELOW;
+        // short texts and reduced strings under 1 Gi symbols by prefix
+        // doubling (fewer round trips than recursion), 16-item tiles
+        d.finish_below = width == 1 ? PSACAK_DEFAULT_FINISH_BELOW : PSACAK_DEFAULT_FINISH_BELOW32;
         d.inner_finish_below = PSACAK_DEFAULT_INNER_FINISH_BELOW;
         d.tile_items = PSACAK_DEFAULT_TILE_ITEMS;
     }
@@ -675,7 +677,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
                  const psacak_schedule *sched) {
     PSK_CUDA(cudaSetDevice(c.dev.id));
     c.stream = stream ? stream : c.own_stream;
-    apply_schedule(c, sched);
+    apply_schedule(c, sched, (int)sizeof(C));
     c.trace.clear();
     c.pending_hash.clear();
     PSK_TRY(c.arena_prepare());
@@ -996,7 +998,7 @@ int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *o
     Ctx &c = ctx->c;
     PSK_CUDA(cudaSetDevice(c.dev.id));
     c.stream = stream ? (cudaStream_t)stream : c.own_stream;
-    apply_schedule(c, sched);
+    apply_schedule(c, sched, 1);
     c.trace.clear();
     c.pending_hash.clear();
     PSK_TRY(c.arena_prepare());
@@ -1221,7 +1223,7 @@ int psacak_debug_reduced8(psacak_ctx *ctx, const uint8_t *d_text, uint64_t n, ui
     Ctx &c = ctx->c;
     PSK_CUDA(cudaSetDevice(c.dev.id));
     c.stream = c.own_stream;
-    apply_schedule(c, sched);
+    apply_schedule(c, sched, 1);
     c.trace.clear();
     c.pending_hash.clear();
     c.debug_red = d_red;

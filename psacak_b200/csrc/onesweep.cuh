@@ -62,16 +62,18 @@ __device__ __forceinline__ void os_store(uint64_t *p, uint64_t v) {
 // Publishes this tile's count of digit d and returns the digit's exclusive
 // prefix over all earlier tiles: walks back over aggregates until a tile
 // with an inclusive prefix, then publishes its own inclusive prefix.  Each
-// poll of a not-yet-ready word counts against OS_SPIN_LIMIT.
-template <int WINDOW = OS_LB_WINDOW>
+// poll of a not-yet-ready word counts against OS_SPIN_LIMIT.  PUBLISHED:
+// the caller has already published the count (an aggregate, or for tile 0
+// its prefix), so only the walk and the final prefix remain.
+template <int WINDOW = OS_LB_WINDOW, bool PUBLISHED = false>
 __device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile, uint32_t d, uint32_t count,
                                                 uint32_t epoch, uint32_t *err) {
     uint64_t *my = status + (uint64_t)tile * 256 + d;
     if (tile == 0) {
-        os_store(my, os_word(epoch, OS_FLAG_PREFIX, count));
+        if (!PUBLISHED) os_store(my, os_word(epoch, OS_FLAG_PREFIX, count));
         return 0;
     }
-    os_store(my, os_word(epoch, OS_FLAG_AGG, count));
+    if (!PUBLISHED) os_store(my, os_word(epoch, OS_FLAG_AGG, count));
     uint32_t excl = 0;
     int64_t t = (int64_t)tile - 1;
     uint32_t left = 0;  // poll budget (spin_spend)

@@ -98,7 +98,7 @@ def main(argv=None):
     picks = np.array([net.predict(x)[0] for x in X[te]])
     report = {"texts": len(X), "train": len(tr), "held_out": len(te), "autotune_seconds": t_tune,
               "loss_first": hist[0], "loss_last": hist[-1], "best_fixed_index": best_fixed,
-              "best_fixed_schedule": sel.SCHEDULES[best_fixed], "library_default": sel.LIBRARY_DEFAULT,
+              "best_fixed_schedule": sel.SCHEDULES[best_fixed], "library_default": {"u8": sel.library_default(1), "u32": sel.library_default(4)},
               "schedules": sel.SCHEDULES}
     report.update(evaluate(T[te], D[te], picks, best_fixed))
     # the same comparison over all texts (the network saw three quarters of them)

@@ -48,7 +48,9 @@ def _u32(t):
     return t.cpu().numpy().view(np.uint32)
 
 
-DEFAULT_FINISH = (1 << 26, 1 << 30)  # PSACAK_DEFAULT_FINISH_BELOW, PSACAK_DEFAULT_INNER_FINISH_BELOW
+# PSACAK_DEFAULT_FINISH_BELOW (bytes) or _BELOW32 (integers), PSACAK_DEFAULT_INNER_FINISH_BELOW
+DEFAULT_FINISH8 = (1 << 24, 1 << 30)
+DEFAULT_FINISH32 = (1 << 26, 1 << 30)
 
 
 def _levels_match(got, want, finish):
@@ -75,7 +77,7 @@ def test_genome_1gib_matches_oracle(ctx):
     ds = torch.empty(n, dtype=torch.int32, device="cuda")
     ctx.psacak8_dev(dt.data_ptr(), n, ds.data_ptr(), stream, None)
     torch.cuda.synchronize()
-    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH)
+    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH8)
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     assert ctx.check_sa8_dev(dt.data_ptr(), n, ds.data_ptr(), stream)
     # induced sorting down to 64 Mi symbols, the old default's shape
@@ -110,7 +112,7 @@ def test_zipf32_256m_matches_oracle(ctx):
     torch.cuda.synchronize()
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     # the levels the default schedule recursed through are the oracle's
-    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH)
+    _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH32)
     ds.zero_()
     ctx.psacak32_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {})  # zero schedule: no finisher
     torch.cuda.synchronize()
