@@ -655,6 +655,14 @@ struct ProfGuard {
     ~ProfGuard() { t_prof = nullptr; }
 };
 
+// The bucket scans count their scattered entries on the device in every
+// build; a profiled call starts that count from zero so that it covers its
+// own build only.
+static status_t profile_begin(Ctx &c) {
+    if (c.profiling) PSK_CUDA(cudaMemsetAsync(c.d_induced, 0, sizeof(unsigned long long), c.stream));
+    return PSACAK_OK;
+}
+
 // Folds the device-side count of entries scattered by the bucket scans into
 // the "induce_scatter" class (per entry: the entry and its predecessor
 // window written, 8 bytes, and one text byte read in front of it).
@@ -687,6 +695,7 @@ status_t run_dev(Ctx &c, const C *d_text, uint64_t n, uint32_t *d_sa, cudaStream
         c.stage_t0 = 0;
     }
     ProfGuard pg(c);
+    PSK_TRY(profile_begin(c));
     status_t st;
     if constexpr (sizeof(C) == 1) st = build_level<uint8_t>(c, d_text, nullptr, nullptr, 256, n, d_sa, 0);
     else st = build_psacak32(c, d_text, n, d_sa);
@@ -1003,6 +1012,7 @@ int psacak8_batch_dev(psacak_ctx *ctx, const uint8_t *d_texts, const uint64_t *o
     c.pending_hash.clear();
     PSK_TRY(c.arena_prepare());
     ProfGuard pg(c);
+    PSK_TRY(profile_begin(c));
     status_t st = build_batch(c, d_texts, offsets, n_texts, d_sas);
     if (st != PSACAK_OK) return c.fail(st);
     PSK_TRY(c.sync());

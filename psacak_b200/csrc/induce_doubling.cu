@@ -175,22 +175,11 @@ template <class C, bool STYPE> struct WEmit {
     }
 };
 
-// Recursion finisher: every position is an item, grouped by its symbol's
-// bucket (head from the bucket boundaries), terminated only by the sentinel.
-struct AllPred {
-    __device__ __forceinline__ bool operator()(uint64_t) const { return true; }
-};
-struct AllEmit {
-    const uint32_t *names, *bheads;
-    uint32_t *Wg, *Wv, *R;
-    __device__ __forceinline__ void operator()(uint64_t j, uint32_t slot) const {
-        uint32_t id = names[j];
-        Wg[slot] = id;
-        Wv[slot] = (uint32_t)j;
-        R[j] = bheads[id] + 1;
-    }
-};
-__global__ void k_copy_heads(const uint32_t *bheads, uint64_t nbuckets, uint32_t *gstart) {
+// Group starts of a whole-string sort's first round (the bucket heads), and
+// the item count where the rounds read it on the device.
+__global__ void k_copy_heads(const uint32_t *bheads, uint64_t nbuckets, uint32_t *gstart, uint32_t *dcount,
+                             uint32_t n) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dcount = n;
     for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nbuckets; c += (uint64_t)gridDim.x * blockDim.x)
         gstart[c] = bheads[c];
 }
@@ -245,6 +234,46 @@ __global__ void __launch_bounds__(256) k_keys(const uint32_t *__restrict__ Wg, c
             }
             radix_count_digits(sh, key, valid, 0, npasses, nbits);
         }
+    }
+    __syncthreads();
+    radix_flush_digits(sh, npasses, hist);
+}
+
+// Keys of the first round of a whole-string sort, where every position j is
+// an item (item j = position j): the group (the name of j) above the names
+// of j + 1 .. j + P - 1, each + 1 in NB bits (0 at and past the end of the
+// string).  These order the suffixes by their first P symbols, so the round
+// after it doubles from h = P instead of h = 1: the early rounds, in which
+// nearly every item is still unresolved, run fewer times.  The kernel also
+// gives every position its first rank, the slot of its bucket's head + 1.
+// Digits are counted as in k_keys.
+__global__ void __launch_bounds__(256) k_keys_packed(const uint32_t *__restrict__ names,
+                                                     const uint32_t *__restrict__ bheads, uint64_t n, int P, int NB,
+                                                     uint64_t *keys, uint32_t *vals, uint32_t *R, int nbits,
+                                                     uint32_t *hist) {
+    __shared__ uint32_t sh[RADIX_MAX_PASSES * 256];
+    const int npasses = (nbits + 7) / 8;
+    const int KB = (P - 1) * NB;
+    for (int i = threadIdx.x; i < npasses * 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t ib = (uint64_t)blockIdx.x * blockDim.x; ib < n; ib += stride) {
+        const uint64_t j = ib + threadIdx.x;
+        const bool valid = j < n;
+        uint64_t key = 0;
+        if (valid) {
+            const uint32_t g = names[j];
+            uint64_t r = 0;
+            for (int t = 1; t < P; t++) {
+                const uint64_t q = j + t;
+                r = (r << NB) | (q < n ? names[q] + 1u : 0u);
+            }
+            key = ((uint64_t)g << KB) | r;
+            keys[j] = key;
+            vals[j] = (uint32_t)j;
+            R[j] = bheads[g] + 1;
+        }
+        radix_count_digits(sh, key, valid, 0, npasses, nbits);
     }
     __syncthreads();
     radix_flush_digits(sh, npasses, hist);
@@ -322,9 +351,227 @@ struct RoundStore {
     }
 };
 
+// ---- rounds over a work list ordered by group ----------------------------
+//
+// Every round after a list's first reads the list that the previous round's
+// scan wrote, in sorted order, so the items of a group are contiguous and
+// groups follow one another in key order.  Only the ranks inside each group
+// need sorting.  Past the first few rounds nearly all groups are a handful of
+// items, so a CTA sorts the small groups that start in its tile in shared
+// memory (each item's slot = the group's start + the items of the group with
+// a smaller (rank, index)), and the items of groups larger than SEG_MAX go
+// through a compaction, the radix sort and a scatter back into place.  The
+// output is the same (key, position) sequence as a full sort up to the order
+// of equal keys, which the scan that follows does not depend on.
+constexpr int SEG_BLOCK = 256;
+constexpr int SEG_TILE = 2048;  // list items whose groups a CTA decides
+constexpr int SEG_MAX = 64;     // largest group sorted in shared memory
+constexpr int SEG_WIN = SEG_TILE + 2 * SEG_MAX;
+constexpr int SEG_WORDS = (SEG_WIN + 1 + 31) / 32;
+constexpr int SEG_OWN = SEG_TILE + SEG_MAX;  // items of the groups a CTA owns
+constexpr int SEG_STEPS = (SEG_OWN + SEG_BLOCK - 1) / SEG_BLOCK;
+// Use the in-place path when the previous round left at most this many
+// items per kept group on average.
+constexpr uint32_t SEG_AVG_MAX = 16;
+
+// Highest set bit of the boundary bitmap in [lo, x], or -1.
+__device__ __forceinline__ int seg_prev(const uint32_t *bm, int x, int lo) {
+    int w = x >> 5;
+    uint32_t m = bm[w] & (0xFFFFFFFFu >> (31 - (x & 31)));
+    while (true) {
+        if (m) {
+            const int p = (w << 5) + 31 - __clz(m);
+            return p >= lo ? p : -1;
+        }
+        if ((w << 5) <= lo) return -1;
+        m = bm[--w];
+    }
+}
+// Lowest set bit of the boundary bitmap in [x + 1, hi], or -1.
+__device__ __forceinline__ int seg_next(const uint32_t *bm, int x, int hi) {
+    const int p0 = x + 1;
+    if (p0 > hi) return -1;
+    int w = p0 >> 5;
+    uint32_t m = bm[w] & (0xFFFFFFFFu << (p0 & 31));
+    while (true) {
+        if (m) {
+            const int p = (w << 5) + __ffs(m) - 1;
+            return p <= hi ? p : -1;
+        }
+        if (((w + 1) << 5) > hi) return -1;
+        m = bm[++w];
+    }
+}
+
+// Keys of one round over a group-ordered list (see above).  CTA b decides
+// the list items [t0, t1) = [b * SEG_TILE, ...): it reads the group ids of
+// the window [t0 - SEG_MAX - 1, t1 + SEG_MAX), marks where groups start, and
+//  * sorts every group of at most SEG_MAX items that starts in [t0, t1)
+//    (such a group ends before t1 + SEG_MAX),
+//  * writes the items of [t0, t1) that belong to larger groups in place and
+//    flags them in `big` (a group whose start lies more than SEG_MAX items
+//    back, or whose end lies more than SEG_MAX items ahead, is large),
+//  * adds its flagged items to *bigcnt.
+// Items of small groups that start before t0 belong to the previous CTA.
+__global__ void __launch_bounds__(SEG_BLOCK) k_seg_keys(const uint32_t *__restrict__ Wg,
+                                                        const uint32_t *__restrict__ Wv, uint64_t cnt,
+                                                        const uint32_t *__restrict__ R, uint64_t n, uint64_t h,
+                                                        int KB, uint64_t *keys, uint32_t *vals, uint8_t *big,
+                                                        uint32_t *bigcnt, uint32_t *err) {
+    __shared__ uint32_t s_g[SEG_WIN + 1];  // s_g[x + 1] = Wg[wlo + x]; s_g[0] = Wg[wlo - 1]
+    __shared__ uint32_t s_bm[SEG_WORDS];   // bit x: list item wlo + x starts a group (x == L: the list's end)
+    __shared__ uint32_t s_r[SEG_OWN], s_v[SEG_OWN];
+    __shared__ uint32_t s_red[33];
+    const uint64_t t0 = (uint64_t)blockIdx.x * SEG_TILE;
+    const uint64_t t1 = t0 + SEG_TILE < cnt ? t0 + SEG_TILE : cnt;
+    const uint64_t wlo = t0 > (uint64_t)SEG_MAX ? t0 - SEG_MAX : 0;
+    const uint64_t whi = t1 + SEG_MAX < cnt ? t1 + SEG_MAX : cnt;
+    const int L = (int)(whi - wlo);
+    const int xt0 = (int)(t0 - wlo), xt1 = (int)(t1 - wlo);
+    for (int x = threadIdx.x; x <= L; x += SEG_BLOCK) {
+        if (x == 0) s_g[0] = wlo > 0 ? Wg[wlo - 1] : 0xFFFFFFFFu;
+        else s_g[x] = Wg[wlo + x - 1];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (L + 1 + 31) >> 5;
+    for (int base = warp * 32; base < nw * 32; base += SEG_BLOCK) {  // warp-uniform
+        const int x = base + lane;
+        bool b = false;
+        if (x < L) b = (wlo + x == 0) || s_g[x + 1] != s_g[x];
+        else if (x == L) b = whi == cnt;
+        const uint32_t m = __ballot_sync(FULL_MASK, b);
+        if (lane == 0) s_bm[base >> 5] = m;
+    }
+    __syncthreads();
+    // each owned or flagged item: its rank gather
+    int ga[SEG_STEPS], gb[SEG_STEPS];
+    uint32_t nbig = 0;
+#pragma unroll
+    for (int u = 0; u < SEG_STEPS; u++) {
+        const int x = xt0 + u * SEG_BLOCK + (int)threadIdx.x;
+        ga[u] = -1;
+        gb[u] = -1;
+        if (x >= L) continue;
+        const int lo = x - SEG_MAX + 1 > 0 ? x - SEG_MAX + 1 : 0;
+        const int a = seg_prev(s_bm, x, lo);
+        const int b = a >= 0 ? seg_next(s_bm, x, a + SEG_MAX < L ? a + SEG_MAX : L) : -1;
+        const bool small = b >= 0;
+        const bool owned = small && a >= xt0 && a < xt1;
+        const bool flagged = !small && x < xt1;
+        if (x < xt1) big[wlo + x] = flagged ? 1 : 0;
+        if (!owned && !flagged) continue;
+        const uint32_t v = Wv[wlo + x];
+        const uint64_t q = (uint64_t)v + h;
+        uint32_t r = 0;
+        if (q <= n) r = R[q];
+        else dev_fail(err, DEVERR_RANGE);
+        s_r[x - xt0] = r;
+        s_v[x - xt0] = v;
+        if (owned) {
+            ga[u] = a;
+            gb[u] = b;
+        } else {
+            keys[wlo + x] = ((uint64_t)s_g[x + 1] << KB) | r;
+            vals[wlo + x] = v;
+            nbig++;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < SEG_STEPS; u++) {
+        if (ga[u] < 0) continue;
+        const int x = xt0 + u * SEG_BLOCK + (int)threadIdx.x;
+        const uint32_t r = s_r[x - xt0];
+        int less = 0;
+        for (int y = ga[u]; y < gb[u]; y++) {
+            const uint32_t ry = s_r[y - xt0];
+            less += (ry < r || (ry == r && y < x)) ? 1 : 0;
+        }
+        const uint64_t p = wlo + (uint64_t)(ga[u] + less);
+        keys[p] = ((uint64_t)s_g[x + 1] << KB) | r;
+        vals[p] = s_v[x - xt0];
+    }
+    uint32_t tot = 0;
+    block_exclusive_sum<uint32_t, SEG_BLOCK>(nbig, s_red, &tot);
+    if (threadIdx.x == 0 && tot) atomicAdd(bigcnt, tot);
+}
+
+// The flagged items, in list order, with their list index.
+struct BigPred {
+    const uint8_t *big;
+    __device__ __forceinline__ bool operator()(uint64_t i) const { return big[i] != 0; }
+};
+struct BigEmit {
+    const uint64_t *keys;
+    const uint32_t *vals;
+    uint64_t *bk;
+    uint32_t *bv, *src;
+    __device__ __forceinline__ void operator()(uint64_t i, uint32_t slot) const {
+        bk[slot] = keys[i];
+        bv[slot] = vals[i];
+        src[slot] = (uint32_t)i;
+    }
+};
+// The sorted flagged items back into the list.  A large group's items were
+// gathered in list order and sort to a contiguous run of the same length,
+// so the q-th sorted item takes the list index of the q-th gathered one.
+__global__ void k_seg_back(const uint64_t *__restrict__ bk, const uint32_t *__restrict__ bv,
+                           const uint32_t *__restrict__ src, uint64_t nb, uint64_t cnt, uint64_t *keys,
+                           uint32_t *vals, uint32_t *err) {
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nb; q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = src[q];
+        if (i >= cnt) {
+            dev_fail(err, DEVERR_RANGE);
+            continue;
+        }
+        keys[i] = bk[q];
+        vals[i] = bv[q];
+    }
+}
+
+// Keys of a group-ordered round (k_seg_keys, then the large groups' sort).
+static status_t seg_round_keys(Ctx &ctx, const uint32_t *Wg, const uint32_t *Wv, uint64_t cnt, const uint32_t *R,
+                               uint64_t n, uint64_t h, int KB, int GB, uint64_t *keys, uint32_t *vals,
+                               cudaStream_t s) {
+    uint32_t *d_big = ctx.d_scalars + 13;
+    DBuf<uint8_t> big;
+    PSK_TRY(big.init(ctx, cnt));
+    PSK_CUDA(cudaMemsetAsync(d_big, 0, sizeof(uint32_t), s));
+    const uint64_t g = ceil_div(cnt, SEG_TILE);
+    PSK_PROF_LAUNCH(s, "double_seg_keys", cnt, 21ull * cnt,
+                    (k_seg_keys<<<(uint32_t)g, SEG_BLOCK, 0, s>>>(Wg, Wv, cnt, R, n, h, KB, keys, vals, big, d_big,
+                                                                  ctx.d_err)));
+    PSK_LAUNCH_CHECK();
+    uint32_t nb = 0;
+    PSK_TRY(ctx.read_u32(d_big, &nb));
+    if (ctx.stage_timing)
+        fprintf(stderr, "[psacak]   group-ordered round h=%llu: %llu items, %u in groups over %d\n",
+                (unsigned long long)h, (unsigned long long)cnt, nb, SEG_MAX);
+    if (nb == 0) return PSACAK_OK;
+    DBuf<uint64_t> bk0, bk1;
+    DBuf<uint32_t> bv0, bv1, src;
+    PSK_TRY(bk0.init(ctx, nb));
+    PSK_TRY(bk1.init(ctx, nb));
+    PSK_TRY(bv0.init(ctx, nb));
+    PSK_TRY(bv1.init(ctx, nb));
+    PSK_TRY(src.init(ctx, nb));
+    PSK_TRY(ctx.compact(BigPred{big}, BigEmit{keys, vals, bk0, bv0, src}, cnt, ctx.d_scalars + 14, "seg_gather"));
+    int in1 = 0;
+    PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(bk0, bv0, bk1, bv1, nb, 0, KB + GB, &in1)));
+    const uint64_t gg = ceil_div(nb, 256);
+    PSK_PROF_LAUNCH(s, "seg_back", nb, 28ull * nb,
+                    (k_seg_back<<<(uint32_t)(gg < 16384 ? gg : 16384), 256, 0, s>>>(
+                        in1 ? bk1.get() : bk0.get(), in1 ? bv1.get() : bv0.get(), src, nb, cnt, keys, vals,
+                        ctx.d_err)));
+    PSK_LAUNCH_CHECK();
+    return PSACAK_OK;
+}
+
 static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, const uint32_t *d_cnt0,
                                 uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0,
-                                uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s);
+                                uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, const uint32_t *names1,
+                                const uint32_t *bheads1, char tag, cudaStream_t s);
 
 // One scan (L or S): resolves the chains of every item of the given type.
 template <class C, bool STYPE>
@@ -352,7 +599,8 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
     }
     uint32_t cnt = 0;
     PSK_TRY(ctx.read_u32(d_cnt, &cnt));
-    return doubling_rounds(ctx, n, nbuckets, cnt, d_cnt, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, STYPE ? 'S' : 'L', s);
+    return doubling_rounds(ctx, n, nbuckets, cnt, d_cnt, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, nullptr, nullptr,
+                           STYPE ? 'S' : 'L', s);
 }
 
 // Rounds of a work list shorter than this run DOUBLING_SPEC_ROUNDS at a
@@ -362,6 +610,8 @@ static status_t doubling_scan(Ctx &ctx, const C *text, uint64_t n, const uint32_
 // the block can meet, and every radix pass runs.  A round left with no
 // items costs a handful of empty launches, less than a read-back.
 constexpr uint32_t DOUBLING_SPEC_MAX = 1u << 20;
+// Most symbols packed into the first round's keys (k_keys_packed).
+constexpr int DOUBLING_PACK_MAX = 16;
 constexpr int DOUBLING_SPEC_ROUNDS = 2;
 
 // Rank-doubling rounds over the work list (Wg = dense group id, Wv =
@@ -369,7 +619,8 @@ constexpr int DOUBLING_SPEC_ROUNDS = 2;
 // holding cnt (the work list's count).
 static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_t cnt, const uint32_t *d_cnt0,
                                 uint32_t *R, uint32_t *sa, uint32_t *Wg, uint32_t *Wv, uint64_t *k0, uint32_t *v0,
-                                uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, char tag, cudaStream_t s) {
+                                uint64_t *k1, uint32_t *v1, uint32_t *gA, uint32_t *gB, const uint32_t *names1,
+                                const uint32_t *bheads1, char tag, cudaStream_t s) {
     const int KB = bitlen(n);
     uint64_t ngroups = nbuckets;
     // round totals alternate between two device slots: a round reads its
@@ -397,20 +648,41 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
             const uint64_t gbound = r == 0 ? ngroups : (cnt > 0 ? cnt : 1);
             const int GB = bitlen(gbound > 0 ? gbound - 1 : 0);
             const uint32_t *dc = spec ? dcnt : nullptr;
-            uint64_t gblocks = ceil_div(cnt, 256 * 16);
-            PSK_CUDA(cudaMemsetAsync(ctx.d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
-            PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
-                            (k_keys<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
-                                Wg, Wv, cnt, dc, R, n, h, KB, kA, vA, KB + GB, ctx.d_hist, ctx.d_err)));
-            PSK_LAUNCH_CHECK();
+            // the first round of a whole-string sort keys by packed names:
+            // as many symbols as fit beside the group id in 64 bits
+            const bool packed = h == 1 && names1 && bheads1;
+            const int NB = bitlen(nbuckets);
+            int P = packed ? 1 + (64 - GB) / NB : 1;
+            if (P > DOUBLING_PACK_MAX) P = DOUBLING_PACK_MAX;
+            const int KBr = packed ? (P - 1) * NB : KB;
+            // a list written by the previous round is ordered by group
+            const bool seg = !spec && h > 1 && ngroups > 0 && (uint64_t)cnt <= (uint64_t)SEG_AVG_MAX * ngroups;
             int in1 = 0;
-            PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(kA, vA, kB, vB, cnt, 0, KB + GB, &in1, true, dc)));
+            if (seg) {
+                PSK_TRY(seg_round_keys(ctx, Wg, Wv, cnt, R, n, h, KBr, GB, kA, vA, s));
+            } else {
+                uint64_t gblocks = ceil_div(cnt, 256 * 16);
+                PSK_CUDA(cudaMemsetAsync(ctx.d_hist, 0, RADIX_MAX_PASSES * 256 * sizeof(uint32_t), s));
+                if (packed) {
+                    if (cnt != n) return set_error(PSACAK_EINTERNAL, "doubling: first round over %u of %llu items",
+                                                   cnt, (unsigned long long)n);
+                    PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
+                                    (k_keys_packed<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
+                                        names1, bheads1, n, P, NB, kA, vA, R, KBr + GB, ctx.d_hist)));
+                } else {
+                    PSK_PROF_LAUNCH(s, "double_keys", cnt, 20ull * cnt,
+                                    (k_keys<<<(uint32_t)(gblocks < 1184 ? gblocks : 1184), 256, 0, s>>>(
+                                        Wg, Wv, cnt, dc, R, n, h, KBr, kA, vA, KBr + GB, ctx.d_hist, ctx.d_err)));
+                }
+                PSK_LAUNCH_CHECK();
+                PSK_TRY((ctx.radix_sort<uint64_t, uint32_t>(kA, vA, kB, vB, cnt, 0, KBr + GB, &in1, true, dc)));
+            }
             uint64_t *ks = in1 ? kB : kA, *kfree = in1 ? kA : kB;
             uint32_t *vs = in1 ? vB : vA, *vfree = in1 ? vA : vB;
             Wg = (uint32_t *)kfree;
             Wv = Wg + n;
             Tri *tout = d_tri[tb];
-            PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, gbound, KB, ctx.d_err, dc},
+            PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, gbound, KBr, ctx.d_err, dc},
                                           RoundStore{gB, R, sa, Wg, Wv, n, ctx.d_err}, cnt, tout, OpTri(),
                                           "scan_rounds", dc)));
             kA = ks;
@@ -422,8 +694,9 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
             std::swap(gA, gB);
             if (ctx.stage_timing)
                 fprintf(stderr, "[psacak]   doubling %c-scan h=%llu: <= %u items, %d key bits%s\n", tag,
-                        (unsigned long long)h, cnt, KB + GB, spec ? " (count on the device)" : "");
-            h <<= 1;
+                        (unsigned long long)h, cnt, KBr + GB,
+                        spec ? " (count on the device)" : seg ? " (group-ordered)" : "");
+            h = packed ? (uint64_t)P : h << 1;
         }
         uint32_t tri[4];
         PSK_TRY(ctx.read_u32(dcnt - 2, tri, 4));  // the last round's totals (g, s, k, o)
@@ -486,12 +759,12 @@ status_t sort_by_doubling(Ctx &ctx, const uint32_t *names, const uint32_t *bhead
     uint32_t *Wg = (uint32_t *)k1.get(), *Wv = Wg + n;  // the work list (see doubling_rounds)
     PSK_CUDA(cudaMemsetAsync(R.get() + n, 0, sizeof(uint32_t), s));
     uint64_t gb = ceil_div(nbuckets, 256);
-    k_copy_heads<<<(uint32_t)(gb < 4096 ? gb : 4096), 256, 0, s>>>(bheads, nbuckets, gA);
+    k_copy_heads<<<(uint32_t)(gb < 4096 ? gb : 4096), 256, 0, s>>>(bheads, nbuckets, gA, ctx.d_scalars, (uint32_t)n);
     PSK_KCOUNT();
     PSK_LAUNCH_CHECK();
-    PSK_TRY(ctx.compact(AllPred{}, AllEmit{names, bheads, Wg, Wv, R}, n, ctx.d_scalars, "double_items"));
-    return doubling_rounds(ctx, n, nbuckets, (uint32_t)n, ctx.d_scalars, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB, 'A',
-                           s);
+    // the first round builds its keys and ranks from the names directly
+    return doubling_rounds(ctx, n, nbuckets, (uint32_t)n, ctx.d_scalars, R, sa, Wg, Wv, k0, v0, k1, v1, gA, gB,
+                           names, bheads, 'A', s);
 }
 
 template status_t induce_doubling<uint8_t>(Ctx &, const uint8_t *, uint64_t, const uint32_t *, const uint32_t *,

@@ -69,21 +69,23 @@ def test_text_statistics(ctx):
 
 
 def test_selector_beats_the_best_fixed_schedule(ctx):
-    """What the trained network gains over the method without it.  Long byte
-    texts sort fastest by induced sorting at the top level (a recursion
-    cut-off below their length), long integer texts by prefix doubling from
-    the text (a cut-off above it): the serving mix's timings show both by a
-    factor of about 1.6-1.9.  With byte and integer texts of the same lengths
+    """What the trained network gains over the method without it.  Byte
+    texts with long repeats (genome-like: mutated copies of earlier stretches)
+    sort fastest by induced sorting at the top level (a recursion cut-off
+    below their length): prefix doubling from the text needs a round per
+    doubling of the longest repeat.  Integer texts with short repeats (i.i.d.
+    over 2^16) sort fastest by prefix doubling from the text (a cut-off above
+    their length), done in a few rounds.  With both kinds at the same lengths
     (16..40 Mi symbols) no single schedule suits both, so the best fixed one
     (the smallest total time on the training texts) loses on one kind; the
-    network, reading the symbol width among its statistics, picks per text.
-    Held-out texts: the selector's total time must be below the best fixed
-    schedule's by at least 10%, and picks build the oracle's SA."""
+    network, reading the symbol width and the repeat statistics, picks per
+    text.  Held-out texts: the selector's total time must be below the best
+    fixed schedule's by at least 10%, and picks build the oracle's SA."""
     rng = np.random.default_rng(5)
 
     def text(kind, n, seed):
         if kind == 1:
-            return synth.iid(n, b"ACGT", seed=seed)
+            return synth.genome(n, seed=seed)
         return np.random.default_rng(seed).integers(0, 1 << 16, n, dtype=np.uint32)
 
     def texts(count, seed):
