@@ -424,23 +424,7 @@ def run_b200(args):
     value = world * n / (ms / 1000.0)
 
     # roofline of the dominant kernel: one more build with the event profiler
-    ctx.profile_reset()
-    ctx.profile(True)
-    build()
-    torch.cuda.synchronize(dev)
-    ctx.profile(False)
-    stats = ctx.profile_stats()
-    total_ms = sum(s["ms"] for s in stats)
-    dom = max((s for s in stats if s["bytes"] > 0), key=lambda s: s["ms"])
-    peak, peak_kind = measured_peak_hbm()
-    achieved = dom["bytes"] / (dom["ms"] / 1000.0) / 1e9
-    traffic = dominant_traffic(dom["name"], dom["items"] / max(dom["launches"], 1))
-    roofline = {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                "traffic": traffic, "launches": dom["launches"],
-                "algorithmic_bytes_per_launch": dom["bytes"] / max(dom["launches"], 1),
-                "avg_launch_ms": dom["ms"] / max(dom["launches"], 1),
-                "share_of_profiled_time": dom["ms"] / total_ms if total_ms else None}
+    roofline, stats = _profile_roofline(ctx, build, torch, dev)
     build_bytes = algorithmic_build_bytes(trace)
     build_gbs = build_bytes / (ms / 1000.0) / 1e9
 
@@ -639,15 +623,28 @@ def _profile_roofline(ctx, build, torch, dev):
     ctx.profile(False)
     stats = ctx.profile_stats()
     total_ms = sum(s["ms"] for s in stats)
-    dom = max((s for s in stats if s["bytes"] > 0), key=lambda s: s["ms"])
     peak, peak_kind = measured_peak_hbm()
-    achieved = dom["bytes"] / (dom["ms"] / 1000.0) / 1e9
+
+    def gbs(s):
+        return s["bytes"] / (s["ms"] / 1000.0) / 1e9 if s["bytes"] and s["ms"] else None
+
+    # the dominant kernel is the class with the most device time among those
+    # with an algorithmic byte model; the largest classes are listed beside it
+    dom = max((s for s in stats if s["bytes"] > 0), key=lambda s: s["ms"])
+    achieved = gbs(dom)
+    classes = []
+    for s in sorted(stats, key=lambda s: -s["ms"])[:8]:
+        a = gbs(s)
+        classes.append({"kernel": s["name"], "launches": s["launches"], "ms": s["ms"],
+                        "share": s["ms"] / total_ms if total_ms else None,
+                        "achieved_gbs": a, "frac": a / peak if a else None})
     return {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": dominant_traffic(dom["name"], dom["items"] / max(dom["launches"], 1)),
             "launches": dom["launches"], "algorithmic_bytes_per_launch": dom["bytes"] / max(dom["launches"], 1),
             "avg_launch_ms": dom["ms"] / max(dom["launches"], 1),
-            "share_of_profiled_time": dom["ms"] / total_ms if total_ms else None}, stats
+            "share_of_profiled_time": dom["ms"] / total_ms if total_ms else None,
+            "largest_classes": classes}, stats
 
 
 def measure_batch(args, torch, ctx, dev, dist, world, rank, texts, steps, warmup, tune=True, plain_texts=0,
@@ -1002,6 +999,27 @@ def run_zipf32(args):
     ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
     value = world * n / (ms / 1000.0)
     roofline, _ = _profile_roofline(ctx, build, torch, dev)
+
+    def timed_form(sched, note):
+        """The same build with another schedule, timed as the default form."""
+        for _ in range(max(1, args.warmup)):
+            ctx.psacak32_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, sched)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.psacak32_dev(d_text.data_ptr(), n, d_sa.data_ptr(), stream.cuda_stream, sched)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        fms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1) / args.steps)
+        ok = None if args.no_verify else ctx.check_sa32_dev(d_text.data_ptr(), n, d_sa.data_ptr(),
+                                                            stream.cuda_stream)
+        return {"value": world * n / (fms / 1000.0), "unit": UNIT, "ms_per_step": fms, "schedule": sched,
+                "verified": ok, "levels": [[lv["m"], lv["n_lms"], lv["k"]] for lv in ctx.trace()], "note": note}
+
+    induced = timed_form({"tile_items": 16, "finish_below": 1 << 26, "inner_finish_below": 1 << 30},
+                         "induced sorting (chain doubling) at the top level, prefix doubling from the first "
+                         "reduced string on")
+    zero = timed_form({}, "every field 0: induced sorting and recursion on every level, as the reference")
     e2e = None
     if not args.no_e2e:
         h_text = torch.empty(n, dtype=torch.int32, pin_memory=True)
@@ -1037,7 +1055,8 @@ def run_zipf32(args):
                 "data": "synthetic", "config": workload_config(args), "e2e": e2e, "roofline": roofline,
                 "hbm_gbs_algorithmic_build": algorithmic_build_bytes(trace, 12 * n) / (ms / 1000.0) / 1e9,
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches), "verified": verified,
-                "levels": [[lv["m"], lv["n_lms"], lv["k"]] for lv in trace]}
+                "levels": [[lv["m"], lv["n_lms"], lv["k"]] for lv in trace],
+                "induced_top_level": induced, "zero_schedule": zero}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

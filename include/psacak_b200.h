@@ -47,14 +47,16 @@ extern "C" {
  * inner_finish_below = PSACAK_DEFAULT_INNER_FINISH_BELOW and tile_items =
  * PSACAK_DEFAULT_TILE_ITEMS: shorter texts are sorted directly by prefix
  * doubling, longer ones by induced sorting at the top level and prefix
- * doubling from the first reduced string on.  The cut-offs are the ones
- * with the smallest total time on the texts the schedule selector was
- * trained on (4 KiB..64 MiB; large byte texts sort faster by induced
- * sorting, large integer texts by prefix doubling), and the inner one the
- * fastest measured for a 1 GiB genome-like text.  Every schedule gives the
- * same suffix array; it only changes speed. */
+ * doubling from the first reduced string on.  Measured on a B200 for
+ * 2^20..2^28 symbols: byte texts (genome-like, i.i.d. and Markov ACGT) sort
+ * faster by prefix doubling below about 2^24 bytes and by induced sorting
+ * above; integer texts (i.i.d. over 2^16, Zipf with planted repeats) sort
+ * 1.7x..3x faster by prefix doubling at every length, so the integer
+ * cut-off equals the inner one.  The inner cut-off is the fastest measured
+ * for a 1 GiB genome-like text.  Every schedule gives the same suffix
+ * array; it only changes speed. */
 #define PSACAK_DEFAULT_FINISH_BELOW (1u << 24)
-#define PSACAK_DEFAULT_FINISH_BELOW32 (1u << 26)
+#define PSACAK_DEFAULT_FINISH_BELOW32 (1u << 30)
 #define PSACAK_DEFAULT_INNER_FINISH_BELOW (1u << 30)
 #define PSACAK_DEFAULT_TILE_ITEMS 16u
 typedef struct {

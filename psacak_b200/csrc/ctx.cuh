@@ -225,10 +225,12 @@ struct Ctx {
     ScanEnv scan_env() { return ScanEnv{&ss, &os, d_err}; }
     // Single-pass scan (see lbscan.cuh) over n items.
     // `dn` (nullable): the item count is on the device, n is its bound.
+    // `bytes`: algorithmic bytes of the launch for the profiler (0: no model).
     template <class T, class Op, class Load, class Store>
-    status_t scan(Load ld, Store st, uint64_t n, T *total_out, Op op, const char *name, const uint32_t *dn = nullptr) {
+    status_t scan(Load ld, Store st, uint64_t n, T *total_out, Op op, const char *name, const uint32_t *dn = nullptr,
+                  uint64_t bytes = 0) {
         PSK_TRY(ensure_scan(n));
-        return lb_scan<T, Op>(ld, st, n, total_out, op, ss, os, d_err, stream, name, dn);
+        return lb_scan<T, Op>(ld, st, n, total_out, op, ss, os, d_err, stream, name, dn, bytes);
     }
     // Stable LSD radix sort of (key, value) pairs on bits [b0, b1); the
     // sorted data ends in (k1, v1) when *in1 is set, else in (k0, v0).

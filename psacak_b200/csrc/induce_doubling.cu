@@ -319,6 +319,10 @@ struct RoundLoad {
         return t;
     }
 };
+// Algorithmic bytes of the round scan per item: its key and position read
+// (12), its new rank written (4) and, for a kept item, its work-list entry
+// written (8; a resolved item writes its 4-byte slot instead).
+constexpr uint64_t ROUND_SCAN_BYTES = 24;
 struct RoundStore {
     uint32_t *gnext;  // kept subgroup ordinal -> first slot (next round)
     uint32_t *R, *sa, *Wg, *Wv;
@@ -684,7 +688,7 @@ static status_t doubling_rounds(Ctx &ctx, uint64_t n, uint64_t nbuckets, uint32_
             Tri *tout = d_tri[tb];
             PSK_TRY((ctx.scan<Tri, OpTri>(RoundLoad{ks, vs, gA, cnt, n, gbound, KBr, ctx.d_err, dc},
                                           RoundStore{gB, R, sa, Wg, Wv, n, ctx.d_err}, cnt, tout, OpTri(),
-                                          "scan_rounds", dc)));
+                                          "scan_rounds", dc, ROUND_SCAN_BYTES * (uint64_t)cnt)));
             kA = ks;
             vA = vs;
             kB = kfree;

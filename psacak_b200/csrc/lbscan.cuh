@@ -186,9 +186,11 @@ __global__ void __launch_bounds__(LS_BLOCK) k_lbscan(Load ld, Store st, uint64_t
 // Runs the scan; `total_out` (device, nullable) receives the aggregate of
 // all items (the identity when n == 0).
 // `dn` (nullable): the item count is read on the device (at most n).
+// `bytes`: the launch's algorithmic bytes for the profiler (0: no model).
 template <class T, class Op, class Load, class Store>
 status_t lb_scan(Load ld, Store st, uint64_t n, T *total_out, Op op, ScanScratch &ss, OnesweepScratch &os,
-                 uint32_t *err, cudaStream_t s, const char *pname = "scan", const uint32_t *dn = nullptr) {
+                 uint32_t *err, cudaStream_t s, const char *pname = "scan", const uint32_t *dn = nullptr,
+                 uint64_t bytes = 0) {
     if (n == 0) {
         if (total_out) PSK_CUDA(cudaMemsetAsync(total_out, 0, sizeof(T), s));
         return PSACAK_OK;
@@ -200,7 +202,7 @@ status_t lb_scan(Load ld, Store st, uint64_t n, T *total_out, Op op, ScanScratch
     if (os.epoch == 0) os.epoch = 1;
     uint32_t *ticket = os.tickets + (os.epoch & 63);
     PSK_CUDA(cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s));
-    PSK_PROF_LAUNCH(s, pname, n, 0,
+    PSK_PROF_LAUNCH(s, pname, n, bytes,
                     (k_lbscan<T, Op, Load, Store><<<(uint32_t)ntiles, LS_BLOCK, 0, s>>>(
                         ld, st, n, op, ss.flags, ticket, os.epoch, (uint32_t)ntiles, total_out, err, dn)));
     PSK_LAUNCH_CHECK();

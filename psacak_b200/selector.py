@@ -45,7 +45,7 @@ def library_default(width):
     """The schedule a NULL psacak_schedule stands for (include/psacak_b200.h):
     the cut-off depends on the symbol width."""
     return {"engine": ENGINE_BUCKET, "inner_engine": ENGINE_DOUBLING, "tile_items": 16,
-            "finish_below": 1 << 24 if width == 1 else 1 << 26, "inner_finish_below": INNER_FINISH}
+            "finish_below": 1 << 24 if width == 1 else 1 << 30, "inner_finish_below": INNER_FINISH}
 
 
 def _bind():

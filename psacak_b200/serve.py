@@ -22,7 +22,8 @@ is measured per request by wall clock from its arrival time to the moment
 its suffix array is in host memory.
 
 The arrival rate is `load` x the capacity measured first with the same
-workers kept busy (closed loop over the first requests of the plan).
+workers kept busy (closed loop over the first requests of the plan, after
+one untimed pass over the same requests).
 Regret against exhaustive autotuning over every schedule is measured
 afterwards on a sample of the requests, for the selector's picks, the best
 fixed schedule of the training data, and the library's default schedule.
@@ -162,9 +163,13 @@ def run(net, count=20000, seed=5, load=0.7, workers=2, autotune_sample=200, lo=4
     for wk in ws:
         for n, c, s in plan[:4]:
             wk.serve(pool.text(n, c, s), width_of(c))
-    # capacity with every worker busy
+    # capacity with every worker busy: the probe requests twice, the first
+    # pass loading every kernel the picks use and growing each worker's
+    # workspace to the probe's largest request, the second one timed
     pr = plan[:min(probe, count)]
-    secs = _closed_loop(ws, [(pool.text(n, c, s), width_of(c)) for n, c, s in pr])
+    items = [(pool.text(n, c, s), width_of(c)) for n, c, s in pr]
+    _closed_loop(ws, items)
+    secs = _closed_loop(ws, items)
     capacity = len(pr) / secs
     lam = load * capacity
     rng = np.random.default_rng(seed + 7)

@@ -8,8 +8,10 @@ reduced to a hash, and its per-level records).
   `psacak_inplace` shape); SA hash and every level's (m, LMS count, name
   count, reduced-string hash).
 * psacak32 on 2^28 Zipf symbols over 2^20 with planted repeats (seed 2):
-  the default schedule, and the zero schedule whose recursion goes all the
-  way down as the oracle's does (trace compared level by level).
+  the default schedule (prefix doubling from the text), induced sorting at
+  the top level with prefix doubling below, and the zero schedule whose
+  recursion goes all the way down as the oracle's does (trace compared
+  level by level).
 * the 4096-text batch (seed 2): every text's SA hash, with the library's
   default schedule and with a chunked schedule of the kind the autotuner
   picks.
@@ -50,7 +52,7 @@ def _u32(t):
 
 # PSACAK_DEFAULT_FINISH_BELOW (bytes) or _BELOW32 (integers), PSACAK_DEFAULT_INNER_FINISH_BELOW
 DEFAULT_FINISH8 = (1 << 24, 1 << 30)
-DEFAULT_FINISH32 = (1 << 26, 1 << 30)
+DEFAULT_FINISH32 = (1 << 30, 1 << 30)
 
 
 def _levels_match(got, want, finish):
@@ -113,6 +115,13 @@ def test_zipf32_256m_matches_oracle(ctx):
     assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     # the levels the default schedule recursed through are the oracle's
     _levels_match(ctx.trace(), fx["levels"], DEFAULT_FINISH32)
+    # induced sorting at the top level, prefix doubling from the first reduced string on
+    ds.zero_()
+    ctx.psacak32_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {"tile_items": 16, "finish_below": 1 << 26,
+                                                             "inner_finish_below": 1 << 30})
+    torch.cuda.synchronize()
+    _levels_match(ctx.trace(), fx["levels"], (1 << 26, 1 << 30))
+    assert o.hash_u32(_u32(ds)) == fx["sa_hash"]
     ds.zero_()
     ctx.psacak32_dev(dt.data_ptr(), n, ds.data_ptr(), stream, {})  # zero schedule: no finisher
     torch.cuda.synchronize()
