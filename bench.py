@@ -480,6 +480,21 @@ def run_b200(args):
         zero = {"value": world * n / (zms / 1000.0), "unit": UNIT, "ms_per_step": zms, "schedule": zs,
                 "host_round_trips_per_step": zrt, "verified": zok,
                 "note": "every field 0: induced sorting and recursion on every level, as the reference"}
+    # texts the default sorts by prefix doubling from the text: SACA-K's
+    # induced sorting at the top level (either engine), prefix doubling from
+    # the first reduced string on, timed as the plain form
+    induced = None
+    if not args.single_build and n < (1 << 24):
+        induced = {}
+        for name, eng in (("bucket_engine", 1), ("doubling_engine", 2)):
+            isc = {"engine": eng, "tile_items": 16, "finish_below": 1, "inner_finish_below": 1 << 30}
+            ir0 = ctx.round_trips()
+            ims = timed_steps(isc)
+            irt = (ctx.round_trips() - ir0) // (max(1, args.warmup) + args.steps)
+            iok = None if args.no_verify else ctx.check_sa8_dev(d_text.data_ptr(), n, d_sa.data_ptr(),
+                                                                stream.cuda_stream)
+            induced[name] = {"value": world * n / (ims / 1000.0), "unit": UNIT, "ms_per_step": ims, "schedule": isc,
+                             "host_round_trips_per_step": irt, "verified": iok}
 
     # autotuned form: exhaustive search over the selector's schedules on
     # this text (the selector's fallback and yardstick), timed as above
@@ -582,7 +597,7 @@ def run_b200(args):
             "batched": batched,
             "plain_schedule": {"schedule": sched if sched is not None else "NULL (library default)",
                                "note": "the value above"},
-            "zero_schedule": zero,
+            "zero_schedule": zero, "induced_top_level": induced,
             "hbm_gbs_algorithmic_build": build_gbs,
             "build_algorithmic_bytes": build_bytes,
             "cpu_baseline": cpu, "cpu_baseline_all_cores": cpu_all, "clocks": clk, "gpu_launches": int(launches),
