@@ -221,9 +221,9 @@ PSACAK_API int psacak_profile_get(psacak_ctx *ctx, psacak_kernel_stat *out, uint
  * library (held on every GPU that loads the library until exit), so n above
  * that limit returns PSACAK_EINVAL.  No context is used; `stream` is a
  * cudaStream_t (NULL = default stream) on the current device.  The first call
- * on a device looks up the array's device address and should come before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race.  Returns after the check has finished on `stream`.
+ * on a device looks up the array's device address (cudaGetSymbolAddress).
+ * All calls share the array: calls that overlap on the GPU race.  Returns
+ * after the check has finished on `stream`.
  */
 PSACAK_API int psacak_check_sa8_noalloc(const uint8_t *d_text, uint64_t n, const uint32_t *d_sa, int *ok,
                                         void *stream);

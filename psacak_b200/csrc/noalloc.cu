@@ -13,8 +13,7 @@
 //   word.  Every GPU that loads the library keeps it until the process exits.
 // * Host code cannot use the array's name as a device address: the address
 //   is looked up with cudaGetSymbolAddress once per device, on the first call
-//   made with that device current.  That first call should come before any
-//   stream capture.
+//   made with that device current.
 // * All calls share the array and leave their contents in it.  Each call
 //   clears what must start cleared (the result word and the n entries it
 //   uses) on the caller's stream; calls whose work overlaps on the GPU race.
