@@ -454,6 +454,8 @@ template <bool LSCAN> struct BucketPolicy {
     uint32_t lms_hi;     // index of this bucket's last entry in that list
     uint32_t lms_cap;    // entries of the list
     uint32_t *wins;      // wins[slot] = predecessor window of sa[slot] for every placed entry
+    uint32_t targets[8];  // bit d: digit d can receive entries (buckets with a part of the scan's type)
+    __device__ __forceinline__ bool active(uint32_t d) const { return (targets[d >> 5] >> (d & 31)) & 1u; }
     struct Pre {
         uint32_t x;
         uint32_t w;
@@ -579,10 +581,14 @@ static status_t expand_chains(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint3
 
 // Multisplit of one bucket; the cursors move from cur[0..256) to
 // cur[256..512) (the caller swaps the halves afterwards).
+// `hg`: the level's bucket geometry, which bounds the digits an entry of
+// bucket c can send: larger buckets with an L part (L scan), smaller ones
+// with an S part (S scan), and the extraction digit.
 template <bool LSCAN>
 static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t n, BucketSeq seq, uint8_t c,
                            const uint32_t *cur_in, uint32_t *cur_out, uint32_t *wins, cudaStream_t s,
-                           uint32_t *lms_out = nullptr, uint32_t lms_hi = 0, uint32_t lms_cap = 0) {
+                           const ByteGeom &hg, uint32_t *lms_out = nullptr, uint32_t lms_hi = 0,
+                           uint32_t lms_cap = 0) {
     uint32_t nitems = seq.a_len + seq.b_len;
     if (nitems == 0) {
         k_copy_words<<<1, 256, 0, s>>>(cur_in, cur_out, 256);
@@ -592,7 +598,11 @@ static status_t multisplit(Ctx &ctx, const uint8_t *text, uint32_t *sa, uint64_t
     }
     PSK_TRY(ctx.ensure_onesweep(ceil_div(nitems, 8 * OS_BLOCK) + 1));
     BucketPolicy<LSCAN> pol{text, sa, seq, c, cur_in, cur_out, ctx.d_induced, n, ctx.d_err, lms_out, lms_hi, lms_cap,
-                            wins};
+                            wins, {}};
+    for (uint32_t d = 0; d < 256; d++) {
+        const bool target = LSCAN ? (d > c && hg.lcount[d] > 0) : (d < c && hg.scount[d] > 0);
+        if (target || (!LSCAN && lms_out && d == LMS_DIGIT)) pol.targets[d >> 5] |= 1u << (d & 31);
+    }
     // algorithmic bytes: each entry and its window read (8); inducing
     // entries write entry + window (8, added from the device count) and read
     // the text byte in front of their target (1, with it).
@@ -658,7 +668,7 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
             if (sink) PSK_TRY(ctx.sink_part(head, lc));
         }
         BucketSeq seq{head, lc, tail - lmsc, lmsc, +1};
-        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, wins, s));
+        PSK_TRY(multisplit<true>(ctx, text, sa, n, seq, (uint8_t)c, curL, alt, wins, s, hg));
         std::swap(curL, alt);
     }
     alt = cur2.get() + 256;
@@ -676,8 +686,8 @@ status_t induce_bucket8(Ctx &ctx, const uint8_t *text, uint64_t n, const uint32_
         }
         BucketSeq seq{tail - 1, sc, head + lc - 1, lc, -1};
         const bool extract = mode == INDUCE_LMS_SUBSTRINGS && lms_out && hg.lmscount[c] > 0;
-        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, wins, s, extract ? lms_out : nullptr,
-                                  hg.lmsstart[c] + hg.lmscount[c] - 1, (uint32_t)n1));
+        PSK_TRY(multisplit<false>(ctx, text, sa, n, seq, (uint8_t)c, curS, alt, wins, s, hg,
+                                  extract ? lms_out : nullptr, hg.lmsstart[c] + hg.lmscount[c] - 1, (uint32_t)n1));
         std::swap(curS, alt);
     }
     if (sink) ctx.sink_done = true;

@@ -30,6 +30,7 @@
 #pragma once
 
 #include <type_traits>
+#include <utility>
 
 #include "prims.cuh"
 
@@ -113,6 +114,18 @@ __device__ __forceinline__ uint32_t os_lookback(uint64_t *status, uint32_t tile,
 template <class P, class = void> struct os_two_phase : std::false_type {};
 template <class P> struct os_two_phase<P, std::void_t<typename P::Pre>> : std::true_type {};
 
+// A policy with `bool active(d)` names the digits its items can take (the
+// same for every tile of a launch); the others skip the look-back -- their
+// counts are 0 in every tile -- so a tile polls only for digits that can
+// move.  An item whose digit is not active is recorded as DEVERR_RANGE.
+template <class P, class = void> struct os_has_active : std::false_type {};
+template <class P>
+struct os_has_active<P, std::void_t<decltype(std::declval<const P &>().active(0u))>> : std::true_type {};
+template <class P> __device__ __forceinline__ bool os_active(const P &pol, uint32_t d) {
+    if constexpr (os_has_active<P>::value) return pol.active(d);
+    else return true;
+}
+
 constexpr int os_min_blocks(int at12, int ipt) { return ipt < 12 ? at12 * 12 / ipt : at12; }
 
 template <class Policy, int IPT>
@@ -188,7 +201,9 @@ __global__ void __launch_bounds__(OS_BLOCK, os_min_blocks(Policy::kMinBlocks, IP
         s_wcnt[ww][d] = (uint16_t)count;
         count += c;
     }
-    const uint32_t excl = os_lookback(status, tile, d, count, epoch, err);
+    uint32_t excl = 0;
+    if (os_active(pol, d)) excl = os_lookback(status, tile, d, count, epoch, err);
+    else if (count) dev_fail(err, DEVERR_RANGE);
     uint32_t ex, tot;
     block_scan<uint32_t, OpSum<uint32_t>, OS_BLOCK>(count, OpSum<uint32_t>(), s_scan, &ex, &tot);
     s_tstart[d] = ex;
@@ -271,6 +286,7 @@ template <class Pred, class Emit> struct CompactPolicy {
         }
     }
     static constexpr int kOutSign = 1;
+    __device__ __forceinline__ bool active(uint32_t d) const { return d == 0; }
     __device__ __forceinline__ uint64_t out0(uint32_t) const { return 0; }
     __device__ __forceinline__ void store(uint64_t idx, const Item &it, uint32_t) const { emit((uint64_t)it, (uint32_t)idx); }
     __device__ __forceinline__ void finish(uint32_t d, uint32_t total) const {
