@@ -285,8 +285,16 @@ struct RoundPayload {
     uint32_t val;  // position
     uint32_t gs;   // first slot of the item's group
 };
+// Two phases (see lbscan.cuh): the item's key, its neighbours' keys and its
+// position for every item of the thread first, then the group-start gathers.
+struct RoundPre {
+    uint64_t k, kp, kn;  // this key, the previous one, the next one (see `has`)
+    uint32_t val;
+    uint32_t has;  // bit 0: a previous item exists, bit 1: a next one
+};
 struct RoundLoad {
     using Payload = RoundPayload;
+    using Pre = RoundPre;
     static constexpr int kIPT = 6;
     const uint64_t *keys;
     const uint32_t *vals;
@@ -295,21 +303,27 @@ struct RoundLoad {
     int KB;
     uint32_t *err;
     const uint32_t *dcnt;  // nullable: the item count on the device (cnt bounds it)
-    __device__ __forceinline__ Tri operator()(uint64_t i, RoundPayload &pl) const {
+    __device__ __forceinline__ void pre(uint64_t i, RoundPre &p) const {
         const uint64_t cnt = dcnt ? (*dcnt < this->cnt ? *dcnt : this->cnt) : this->cnt;
-        uint64_t k = keys[i];
+        p.k = keys[i];
+        p.val = vals[i];
+        p.has = (i > 0 ? 1u : 0u) | (i + 1 < cnt ? 2u : 0u);
+        p.kp = (p.has & 1u) ? keys[i - 1] : 0ull;
+        p.kn = (p.has & 2u) ? keys[i + 1] : 0ull;
+    }
+    __device__ __forceinline__ Tri operator()(uint64_t i, const RoundPre &p, RoundPayload &pl) const {
+        const uint64_t k = p.k;
         const uint64_t gid = k >> KB;
-        pl.val = vals[i];
+        pl.val = p.val;
         pl.gs = 0;
         if (gid < ngroups && pl.val < n) pl.gs = gstart[gid];
         else pl.val = 0xFFFFFFFFu;  // reported by the store
         bool gb = true, sb = true, sbn = true;
-        if (i > 0) {
-            uint64_t kp = keys[i - 1];
-            gb = (kp >> KB) != (k >> KB);
-            sb = kp != k;
+        if (p.has & 1u) {
+            gb = (p.kp >> KB) != (k >> KB);
+            sb = p.kp != k;
         }
-        if (i + 1 < cnt) sbn = keys[i + 1] != k;
+        if (p.has & 2u) sbn = p.kn != k;
         Tri t;
         t.g = gb ? (uint32_t)(i + 1) : 0u;
         t.s = sb ? (uint32_t)(i + 1) : 0u;
