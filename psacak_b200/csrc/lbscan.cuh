@@ -83,12 +83,12 @@ template <class T> __device__ __forceinline__ void set_word(T &v, int f, uint32_
 // `dn` (nullable): the item count lives on the device (written by an earlier
 // kernel); the launch covers n_max items and the tiles past the count exit
 // at once (with no items at all, tile 0 writes the identity as the total).
-template <class T, class Op, class Load, class Store>
 // At least 4 CTAs per SM (64 registers a thread): the scans wait on memory,
 // and a fourth CTA's loads in flight are worth more than the registers it
 // takes (the round scans of the 1 GiB build: 36.2 ms, against 36.8 ms at 3
 // CTAs and 76 registers).
 constexpr int LS_MIN_BLOCKS = 4;
+template <class T, class Op, class Load, class Store>
 __global__ void __launch_bounds__(LS_BLOCK, LS_MIN_BLOCKS) k_lbscan(Load ld, Store st, uint64_t n_max, Op op, uint64_t *flags,
                                                      uint32_t *ticket, uint32_t epoch, uint32_t ntiles_max,
                                                      T *total_out, uint32_t *err, const uint32_t *dn) {
