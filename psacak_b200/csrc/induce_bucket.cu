@@ -440,7 +440,11 @@ constexpr uint32_t LMS_DIGIT = 255;
 // when an induced suffix's window has no look-ahead byte left.
 template <bool LSCAN> struct BucketPolicy {
     using Item = uint64_t;
-    static constexpr int kMinBlocks = 3;
+    // 4 CTAs per SM (64 registers; the compiler keeps a few values in local
+    // memory): the scatter waits on its loads and on the look-back, and the
+    // fourth CTA measured 31.1 ms against 33.9 ms at 3 CTAs and 80 registers
+    // for the 1 GiB build's scatters.
+    static constexpr int kMinBlocks = 4;
     const uint8_t *text;
     uint32_t *sa;
     BucketSeq seq;
