@@ -25,3 +25,25 @@ def test_reference_gradients_match_finite_differences():
         e[i] = 1e-3
         fd = (loss_of(p + e) - loss_of(p - e)) / 2e-3
         assert abs(fd - g[i]) <= 2e-2 * max(1.0, abs(fd)), (i, fd, g[i])
+
+
+def test_library_default_matches_the_header():
+    """selector.library_default (the schedule a NULL psacak_schedule stands
+    for, used as the yardstick of the selector's regret) equals the header's
+    default cut-offs and tile size for both symbol widths."""
+    import os
+    import re
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "psacak_b200.h")
+    text = open(hdr).read()
+
+    def define(name):
+        m = re.search(r"#define %s \((\d+)u << (\d+)\)" % name, text) or \
+            re.search(r"#define %s (\d+)u\b" % name, text)
+        assert m, name
+        return int(m.group(1)) << int(m.group(2)) if m.lastindex == 2 else int(m.group(1))
+
+    for width, name in ((1, "PSACAK_DEFAULT_FINISH_BELOW"), (4, "PSACAK_DEFAULT_FINISH_BELOW32")):
+        d = sel.library_default(width)
+        assert d["finish_below"] == define(name), (width, d)
+        assert d["inner_finish_below"] == define("PSACAK_DEFAULT_INNER_FINISH_BELOW")
+        assert d["tile_items"] == define("PSACAK_DEFAULT_TILE_ITEMS")
