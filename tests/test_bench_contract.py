@@ -48,3 +48,37 @@ def test_workload_configs_name_the_workload(workload):
     args = bench.parse()
     cfg = bench.workload_config(args)
     assert cfg["workload"] and "model" not in cfg
+
+
+def test_roofline_names_the_largest_class_with_a_byte_model():
+    """bench._profile_roofline: the dominant kernel is the class with the most
+    device time among those with algorithmic bytes; largest_classes lists the
+    classes by time with their fraction of the peak where they have bytes."""
+    import types
+    import bench
+
+    stats = [dict(name="scan_seeds", launches=4, items=10, bytes=0, ms=50.0),
+             dict(name="radix_pass", launches=10, items=100, bytes=3_000_000_000, ms=40.0),
+             dict(name="scan_rounds", launches=2, items=50, bytes=1_000_000_000, ms=45.0),
+             dict(name="small", launches=1, items=1, bytes=10, ms=0.5)]
+
+    class FakeCtx:
+        def profile_reset(self):
+            pass
+
+        def profile(self, on):
+            pass
+
+        def profile_stats(self):
+            return stats
+
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(synchronize=lambda dev: None))
+    roof, got = bench._profile_roofline(FakeCtx(), lambda: None, fake_torch, None)
+    assert got is stats
+    assert roof["kernel"] == "scan_rounds"  # 45 ms; scan_seeds has more time but no byte model
+    assert abs(roof["achieved"] - 1e9 / 0.045 / 1e9) < 1e-6
+    assert abs(roof["frac"] - roof["achieved"] / roof["peak"]) < 1e-12
+    assert abs(roof["share_of_profiled_time"] - 45.0 / 135.5) < 1e-12
+    names = [c["kernel"] for c in roof["largest_classes"]]
+    assert names == ["scan_seeds", "scan_rounds", "radix_pass", "small"]
+    assert roof["largest_classes"][0]["frac"] is None and roof["largest_classes"][2]["frac"] > 0
